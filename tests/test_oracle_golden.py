@@ -1,0 +1,107 @@
+"""Pins the CPU oracle against the reference's golden vectors and known answers.
+
+Golden: test_data/test_lc.dat of the reference, 500 fluxes written by the C++
+lroche for test_data/test_model.dat at times -0.2..1.2, expose 0.001, ndiv 1;
+the reference's own bound is max relative error < 1e-6 (tests/regression.rs:84-88).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def golden_data(O):
+    t = -0.2 + 1.4 * np.arange(500) / 499
+    return O.make_data(t, expose=0.001, ndiv=1, flux=0.0, ferr=0.0, weight=1.0)
+
+
+def test_oracle_matches_cpp_golden(oracle, test_model_path):
+    m = oracle.Model(test_model_path)
+    r = m.light_curve(golden_data(oracle), scale=False, rdata=False, nthreads=4)
+    g = np.loadtxt(GOLDEN / "test_lc.dat")
+    assert np.array_equal(golden_data(oracle)["time"], g[:, 0])
+    rel = np.abs(r["calc"] - g[:, 2]) / np.abs(g[:, 2])
+    # The golden carries 10 significant digits; observed max ~1.4e-10.
+    assert rel.max() < 1e-9, rel.max()
+
+
+def test_oracle_threading_is_bitwise_stable(oracle, test_model_path):
+    m = oracle.Model(test_model_path)
+    a = m.light_curve(golden_data(oracle), nthreads=1)["calc"]
+    b = m.light_curve(golden_data(oracle), nthreads=8)["calc"]
+    assert np.array_equal(a, b)
+
+
+def test_lagrange_known_answers(oracle):
+    L = oracle.lib()
+    # lagrange.rs:148-152, 172-184
+    assert abs(L.orc_xl1(1.0) - 0.5) < 1e-10
+    assert 0.0 < L.orc_xl1(0.1) < 1.0
+    assert abs(L.orc_xl1(0.5) - L.orc_xl11(0.5, 1.0)) < 1e-10
+    assert abs(L.orc_xl1(0.5) - L.orc_xl12(0.5, 1.0)) < 1e-10
+    assert math.isnan(L.orc_xl1(-1.0))
+
+
+def test_planck_known_answers(oracle):
+    L = oracle.lib()
+    # planck.rs:49-75
+    assert L.orc_planck(500.0, 10000.0) > L.orc_planck(500.0, 5000.0) > 0.0
+    assert L.orc_planck(100.0, 100.0) >= 0.0
+    assert L.orc_dlpdlt(500.0, 10000.0) > 0.0 and L.orc_dlpdlt(500.0, 3000.0) > 0.0
+
+
+def test_numface_table(oracle):
+    # Element counts per latitude resolution (grid.rs:8-46).
+    L = oracle.lib()
+    expect = {20: 540, 40: 2058, 50: 3202, 100: 12724, 200: 50872, 400: 203560}
+    for nlat, n in expect.items():
+        assert L.orc_numface(nlat) == n
+
+
+def test_stream_spot_position(oracle):
+    # The stream reaches the requested radius (stream.rs:82-145) from just inside L1.
+    import ctypes as C
+    out = (C.c_double * 3)()
+    oracle.lib().orc_stream_spot(0.5, 0.3, out)
+    r = math.sqrt(out[0] ** 2 + out[1] ** 2 + out[2] ** 2)
+    assert abs(r - 0.3) < 1e-9
+    assert out[2] == 0.0
+
+
+def test_parse_errors(oracle, tmp_path):
+    text = (GOLDEN / "test_model.dat").read_text()
+    with pytest.raises(oracle.OracleError):
+        oracle.Model(text=text + "\nbogus_param = 1\n")
+    with pytest.raises(oracle.OracleError):
+        oracle.Model(text=text.replace("limb1                = Poly", "limb1 = Quadratic"))
+    with pytest.raises(oracle.OracleError):
+        oracle.Model(text=text + "\nstsp11_long = 10 1 1 0\n")
+    m = oracle.Model(text=text)
+    assert m.get("q") == 0.5 and m.get("pdot") == 0.0
+
+
+def test_chisq_batch_matches_sequential(oracle, test_model_path):
+    # tests/chisq_batch.rs:50-89 (batch == sequential to 1e-10)
+    m = oracle.Model(test_model_path)
+    t = -0.2 + 1.4 * np.arange(100) / 99
+    d = oracle.make_data(t, expose=0.001, ndiv=1, flux=0.0, ferr=1.0, weight=1.0)
+    q0 = m.get("q")
+    offs = [-0.02, 0.0, 0.02]
+    vals = np.array([[q0 + dq, m.get("iangle")] for dq in offs])
+    batch = m.chisq_batch(d, ["q", "iangle"], vals, scale=False, nthreads=3)
+    for i, dq in enumerate(offs):
+        mm = m.clone()
+        mm.set("q", q0 + dq)
+        seq = mm.light_curve(d, scale=False, rdata=True)["chisq"]
+        assert abs(batch[i] - seq) < 1e-10 * max(abs(seq), 1.0)
+
+
+def test_chisq_batch_unphysical_is_nan(oracle, test_model_path):
+    # tests/chisq_batch.rs:92-109
+    m = oracle.Model(test_model_path)
+    t = -0.2 + 1.4 * np.arange(50) / 49
+    d = oracle.make_data(t, flux=0.0, ferr=1.0, weight=1.0)
+    out = m.chisq_batch(d, ["r2"], np.array([[0.99]]))
+    assert np.isnan(out[0])
