@@ -1,0 +1,163 @@
+/*
+ * lcurve_b200.h — C ABI of the B200 light-curve engine (liblcurve_b200.so).
+ *
+ * Drop-in boundary for the light-curve path of scope-ml/lcurve-rs: the flux
+ * sum of every star/disc/edge/bright-spot element over times x exposure
+ * sub-divisions, plus the grid generation and Roche eclipse ray-marching that
+ * feed it.  Everything behind these entry points runs as sm_100a CUDA
+ * kernels; there is no CPU fallback.  A call that cannot get a CUDA device
+ * fails with LCB_ERR_NO_DEVICE.
+ *
+ * Conventions (mirroring the reference's lcuda_* FFI, crates/lcurve-cuda/
+ * kernels/flux_kernel.cu:491-627 and crates/lcurve-cuda/src/error.rs:28-37):
+ *   - every function returns an int status, 0 = LCB_OK; no exceptions or
+ *     aborts cross the ABI;
+ *   - all buffers passed in are caller-owned host memory unless the name says
+ *     "device"; device memory is owned by the context;
+ *   - a context serialises its own calls with an internal mutex, so one
+ *     context may be shared by threads (calls then run one at a time), or
+ *     each thread may own a context.
+ */
+#ifndef LCURVE_B200_H
+#define LCURVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define LCB_OK                 0
+#define LCB_ERR_INVALID        1  /* bad argument (null pointer, bad size)           */
+#define LCB_ERR_PARSE          2  /* model / data file syntax (model.rs:186-442)     */
+#define LCB_ERR_IO             3  /* file cannot be read or written                  */
+#define LCB_ERR_MODEL          4  /* physically invalid model (LcurveError/RocheError)*/
+#define LCB_ERR_CUDA           5  /* CUDA runtime error                              */
+#define LCB_ERR_UNKNOWN_PARAM  6  /* name is not a physical parameter (model.rs:459) */
+#define LCB_ERR_NO_DEVICE      7  /* no usable CUDA device / kernel image            */
+#define LCB_ERR_EMPTY          8  /* no data points                                  */
+#define LCB_ERR_DEVICE_CHECK   9  /* a device-side iteration cap or check tripped    */
+
+typedef struct lcb_ctx lcb_ctx;
+typedef struct lcb_model lcb_model;
+typedef struct lcb_batch lcb_batch;
+
+/* One observation; same fields and meaning as Datum (crates/lcurve/src/
+ * types.rs:207-220).  40 bytes of doubles + ndiv + padding = 48 bytes. */
+typedef struct lcb_datum {
+    double time;    /* mid-exposure time                    */
+    double expose;  /* exposure length (time units)         */
+    double flux;    /* observed flux                        */
+    double ferr;    /* uncertainty                          */
+    double weight;  /* weight factor (<= 0: ignored in chi2)*/
+    int32_t ndiv;   /* exposure sub-divisions               */
+    int32_t _pad;
+} lcb_datum;
+
+/* Scalar part of LcResult (crates/lcurve/src/orchestration.rs:9-28). */
+typedef struct lcb_result {
+    double wdwarf;   /* white dwarf contribution at phase 0.5     */
+    double chisq;    /* weighted chi-squared                      */
+    double wnok;     /* weighted number of points used            */
+    double logg1;    /* flux-weighted log10 g of star 1 (cgs)     */
+    double logg2;    /* flux-weighted log10 g of star 2 (cgs)     */
+    double rv1;      /* volume-averaged radius of star 1          */
+    double rv2;      /* volume-averaged radius of star 2          */
+    double sfac[5];  /* scale factors [star1, disc, edge, spot, star2] */
+} lcb_result;
+
+/* ---- library / errors ---------------------------------------------------- */
+const char* lcb_version(void);
+/* Message of the last failing call on this host thread. */
+const char* lcb_last_error(void);
+/* Number of CUDA devices (reference: lcuda_device_count, flux_kernel.cu:557). */
+int lcb_device_count(int* count);
+
+/* ---- context: device, stream, device arena -------------------------------
+ * Replaces CudaContext::new (crates/lcurve-cuda/src/context.rs:261) and
+ * lcuda_init (flux_kernel.cu:497).  Work is issued on the context's own
+ * stream unless lcb_ctx_set_stream gives another one (cudaStream_t). */
+int  lcb_ctx_create(int device, lcb_ctx** out);
+void lcb_ctx_destroy(lcb_ctx* ctx);
+int  lcb_ctx_set_stream(lcb_ctx* ctx, void* cuda_stream);
+const char* lcb_ctx_last_error(const lcb_ctx* ctx);
+
+/* ---- models (crates/lcurve/src/model.rs) --------------------------------- */
+/* Model::from_file (model.rs:186). */
+int  lcb_model_load(const char* path, lcb_model** out);
+/* Same parser over an in-memory text. */
+int  lcb_model_parse(const char* text, lcb_model** out);
+/* Model::clone. */
+int  lcb_model_clone(const lcb_model* m, lcb_model** out);
+void lcb_model_destroy(lcb_model* m);
+/* Model::set_param_value (model.rs:459-493); LCB_ERR_UNKNOWN_PARAM if the
+ * name is not a physical parameter. */
+int  lcb_model_set_param(lcb_model* m, const char* name, double value);
+/* Model::get_param_value (model.rs:495-532). */
+int  lcb_model_get_param(const lcb_model* m, const char* name, double* value);
+/* Full Pparam record (model.rs:7-13): value, range, dstep, vary, defined. */
+int  lcb_model_get_pparam(const lcb_model* m, const char* name, double* value, double* range,
+                          double* dstep, int* vary, int* defined);
+int  lcb_model_set_pparam(lcb_model* m, const char* name, const double* value, const double* range,
+                          const double* dstep, const int* vary);
+/* Computational parameter (nlat1f, delta_phase, limb1, ...) by its .dat text. */
+int  lcb_model_set_comp(lcb_model* m, const char* name, const char* value);
+int  lcb_model_get_comp(const lcb_model* m, const char* name, char* buf, int buflen);
+/* Name of the i-th physical parameter (declaration order, model.rs:66-137);
+ * NULL when i is out of range. */
+const char* lcb_param_name(int i);
+
+/* ---- data files (crates/lcurve/src/types.rs:229-265) --------------------- */
+int  lcb_read_data(const char* path, lcb_datum** out, int64_t* n);
+void lcb_free_data(lcb_datum* data);
+
+/* ---- light curve ----------------------------------------------------------
+ * light_curve_comp(&Model, &Data, scale, rdata) (orchestration.rs:36-318).
+ * calc_out receives n fluxes; res_out may be NULL. */
+int lcb_light_curve(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
+                    int scale, int rdata, double* calc_out, lcb_result* res_out);
+
+/* ---- batched chi-squared ---------------------------------------------------
+ * chisq_batch(base, data, names, values, scale) (orchestration.rs:329-357)
+ * and chisq_batch_gpu (crates/lcurve-cuda/src/batch.rs:73-80): values is an
+ * (nsets x ndim) row-major array; each row is applied with set_param_value
+ * (unknown names are ignored, as there); a model that fails gives NaN. */
+int lcb_chisq_batch(lcb_ctx* ctx, const lcb_model* base, const lcb_datum* data, int64_t n,
+                    const char* const* names, int ndim, const double* values, int64_t nsets,
+                    int scale, double* chisq_out);
+
+/* Ragged batch (no reference counterpart: the reference shares one Data and
+ * one grid size per batch): model i is evaluated on data[offsets[i] ..
+ * offsets[i+1]).  calc_out (same length as data) and res_out (nmodels) may be
+ * NULL.  Each model is computed with rdata = true. */
+int lcb_chisq_batch_ragged(lcb_ctx* ctx, const lcb_model* const* models, int64_t nmodels,
+                           const lcb_datum* data, const int64_t* offsets, int scale,
+                           double* chisq_out, double* calc_out, lcb_result* res_out);
+
+/* ---- resident batch (repeated evaluation, e.g. MCMC) ----------------------
+ * lcb_batch_create plans a ragged batch and uploads its data once;
+ * lcb_batch_set_params changes physical parameters (names x values, row-major,
+ * one row per model) without re-uploading data; lcb_batch_run evaluates on the
+ * device (the launch sequence is captured once in a CUDA graph and replayed);
+ * lcb_batch_results copies results back.  Changing a parameter that alters an
+ * element count (disc/edge sizes) re-plans the batch transparently. */
+int  lcb_batch_create(lcb_ctx* ctx, const lcb_model* const* models, int64_t nmodels,
+                      const lcb_datum* data, const int64_t* offsets, lcb_batch** out);
+void lcb_batch_destroy(lcb_batch* b);
+int  lcb_batch_set_params(lcb_batch* b, const char* const* names, int ndim, const double* values);
+int  lcb_batch_run(lcb_batch* b, int scale);
+int  lcb_batch_results(lcb_batch* b, double* chisq_out, double* calc_out, lcb_result* res_out);
+/* Work counts of the planned batch: [models, elements, sub-phases,
+ * element-evals, flux work units, roche-eclipsed elements, pad, pad]. */
+int  lcb_batch_stats(const lcb_batch* b, int64_t* out8);
+/* Device time (ms) of each stage of the last lcb_batch_run, measured with
+ * CUDA events on the launching stream: [phase, elements, flux, epilogue]. */
+int  lcb_batch_stage_ms(const lcb_batch* b, double* out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LCURVE_B200_H */

@@ -1,0 +1,621 @@
+// lcb_engine.cu — context, device buffers, batch execution and the C ABI.
+//
+// A batch runs as one launch sequence on the context's stream:
+//   memset(aux, status, counter) -> k_phase -> k_elements -> k_flux -> k_epilogue
+// For a resident batch (lcb_batch_*) the sequence is captured once in a CUDA
+// graph and replayed; only the model table changes between runs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lcurve_b200.h"
+#include "lcb_kernels.cuh"
+#include "lcb_model.h"
+#include "lcb_plan.h"
+
+using lcb::Error;
+
+namespace {
+
+thread_local std::string t_last_error;
+
+int fail(int code, const std::string& msg) {
+    t_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (expr);                                                                    \
+        if (e_ != cudaSuccess) throw Error(LCB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        CUDA_TRY(cudaMalloc(&p, want));
+        cap = want;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// All device storage of one planned batch.
+struct DeviceSet {
+    DevBuf models, segs, bands, rings, eblocks, units, dmodel, dsub0, dsrc, data;
+    DevBuf rec, pos, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter, datum;
+    void release() {
+        for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &units, &dmodel, &dsub0, &dsrc, &data, &rec, &pos,
+                          &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac, &partial, &calc, &results, &counter,
+                          &datum})
+            b->release();
+    }
+};
+
+}  // namespace
+
+struct lcb_model {
+    lcb::Model m;
+};
+
+struct lcb_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::mutex mu;
+    std::string last_error;
+    DeviceSet scratch;  // buffers of transient (non-resident) calls
+    cudaEvent_t ev[5] = {};
+};
+
+struct lcb_batch {
+    lcb_ctx* ctx = nullptr;
+    std::vector<lcb::Model> models;
+    std::vector<lcb_datum> data;
+    std::vector<int64_t> start, count;
+    lcb::Plan plan;
+    DeviceSet dev;
+    cudaGraphExec_t graph = nullptr;
+    int graph_scale = -1;
+    std::vector<int64_t> graph_key;
+    bool ran = false;
+    double stage_ms[4] = {0, 0, 0, 0};
+    std::vector<double> h_results, h_calc;
+    std::vector<int> h_status;
+};
+
+namespace {
+
+// Upload of the plan's tables (and the data) into a device set.
+void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* data, int64_t ndata_src,
+                 bool upload_data) {
+    cudaStream_t s = C->stream;
+    auto put = [&](DevBuf& b, const void* src, size_t bytes) {
+        b.ensure(bytes);
+        if (bytes) CUDA_TRY(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
+    };
+    const int64_t nm = (int64_t)P.models.size();
+    put(D.models, P.models.data(), nm * sizeof(lcb::ModelDev));
+    put(D.segs, P.segs.data(), P.segs.size() * sizeof(lcb::SegDesc));
+    put(D.bands, P.bands.data(), P.bands.size() * sizeof(lcb::Band));
+    put(D.rings, P.rings.data(), P.rings.size() * sizeof(lcb::Ring));
+    put(D.eblocks, P.eblocks.data(), P.eblocks.size() * sizeof(lcb::ElemBlock));
+    put(D.units, P.units.data(), P.units.size() * sizeof(lcb::FluxUnit));
+    put(D.dmodel, P.datum_model.data(), P.datum_model.size() * sizeof(int32_t));
+    put(D.dsub0, P.datum_sub0.data(), P.datum_sub0.size() * sizeof(int64_t));
+    if (upload_data) {
+        // expanded (model, datum) records; shared data is gathered on the host once
+        std::vector<lcb_datum> ex(P.ndatum);
+        for (int64_t d = 0; d < P.ndatum; ++d) ex[d] = data[P.datum_src[d]];
+        (void)ndata_src;
+        put(D.datum, ex.data(), ex.size() * sizeof(lcb_datum));
+    }
+    D.rec.ensure(P.nelem * sizeof(float4));
+    D.pos.ensure(P.nelem * sizeof(float4));
+    D.ecl.ensure(P.nelem * lcb::kMaxEcl * sizeof(double2));
+    D.aux.ensure(nm * lcb::kNumAux * sizeof(double));
+    D.status.ensure(nm * sizeof(int));
+    D.spe.ensure(P.nsub * sizeof(float4));
+    D.spphi.ensure(P.nsub * sizeof(double));
+    D.sptype.ensure(P.nsub * sizeof(int8_t));
+    D.spw.ensure(P.nsub * sizeof(double));
+    D.slfac.ensure(P.ndatum * sizeof(double));
+    D.partial.ensure(P.npartial * sizeof(double));
+    D.calc.ensure(P.ndatum * sizeof(double));
+    D.results.ensure(nm * 12 * sizeof(double));
+    D.counter.ensure(sizeof(int) * 4);
+}
+
+// The device launch sequence of one batch evaluation.
+void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rdata, bool timed) {
+    cudaStream_t s = C->stream;
+    const int64_t nm = (int64_t)P.models.size();
+    CUDA_TRY(cudaMemsetAsync(D.aux.p, 0, nm * lcb::kNumAux * sizeof(double), s));
+    CUDA_TRY(cudaMemsetAsync(D.status.p, 0, nm * sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(D.counter.p, 0, sizeof(int) * 4, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[0], s));
+    lcb::PhaseArgs pa{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dmodel.as<int32_t>(),
+                      D.dsub0.as<int64_t>(), P.ndatum, D.spe.as<float4>(), D.spphi.as<double>(),
+                      D.sptype.as<int8_t>(), D.spw.as<double>(), D.slfac.as<double>()};
+    CUDA_TRY(lcb::launch_phase(pa, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[1], s));
+    lcb::ElemArgs ea{D.models.as<lcb::ModelDev>(), D.segs.as<lcb::SegDesc>(), D.eblocks.as<lcb::ElemBlock>(),
+                     D.bands.as<lcb::Band>(), D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(),
+                     D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(), (int64_t)P.eblocks.size()};
+    CUDA_TRY(lcb::launch_elements(ea, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[2], s));
+    lcb::FluxArgs fa{D.models.as<lcb::ModelDev>(), D.units.as<lcb::FluxUnit>(), (int64_t)P.units.size(),
+                     D.counter.as<int>(), D.rec.as<float4>(), D.pos.as<float4>(), D.ecl.as<double2>(),
+                     D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
+                     D.status.as<int>()};
+    int64_t grid = (int64_t)C->num_sms * lcb::flux_blocks_per_sm();
+    grid = std::min<int64_t>(grid, std::max<int64_t>((int64_t)P.units.size(), 1));
+    CUDA_TRY(lcb::launch_flux(fa, (int)grid, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[3], s));
+    lcb::EpiArgs pe{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dsub0.as<int64_t>(),
+                    D.spphi.as<double>(), D.spw.as<double>(), D.slfac.as<double>(), D.partial.as<double>(),
+                    D.aux.as<double>(), D.status.as<int>(), scale, rdata, D.calc.as<double>(),
+                    D.results.as<double>(), nm};
+    CUDA_TRY(lcb::launch_epilogue(pe, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[4], s));
+}
+
+void set_device(lcb_ctx* C) { CUDA_TRY(cudaSetDevice(C->device)); }
+
+void fetch_results(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, std::vector<double>& res, std::vector<double>* calc,
+                   std::vector<int>* status) {
+    const int64_t nm = (int64_t)P.models.size();
+    res.resize(nm * 12);
+    CUDA_TRY(cudaMemcpyAsync(res.data(), D.results.p, nm * 12 * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    if (calc) {
+        calc->resize(P.ndatum);
+        if (P.ndatum)
+            CUDA_TRY(cudaMemcpyAsync(calc->data(), D.calc.p, P.ndatum * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    }
+    if (status) {
+        status->resize(nm);
+        CUDA_TRY(cudaMemcpyAsync(status->data(), D.status.p, nm * sizeof(int), cudaMemcpyDeviceToHost, C->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(C->stream));
+}
+
+void fill_result(const double* r, lcb_result* out) {
+    out->wdwarf = r[0]; out->chisq = r[1]; out->wnok = r[2]; out->logg1 = r[3]; out->logg2 = r[4];
+    out->rv1 = r[5]; out->rv2 = r[6];
+    for (int k = 0; k < 5; ++k) out->sfac[k] = r[7 + k];
+}
+
+void check_iscale(const lcb::Model& m) {
+    if (m.iscale) throw Error(LCB_ERR_INVALID, "iscale=1 (per-component scale factors) is not supported by this engine yet");
+}
+
+// A transient evaluation on the context's scratch buffers.
+void run_transient(lcb_ctx* C, const lcb::Model* const* models, int64_t n, const lcb_datum* data,
+                   const int64_t* start, const int64_t* count, int scale, int rdata, std::vector<double>& res,
+                   std::vector<double>* calc, lcb::Plan& P, std::vector<int>& st) {
+    for (int64_t i = 0; i < n; ++i) check_iscale(*models[i]);
+    lcb::plan_batch(models, n, data, start, count, C->num_sms, P);
+    upload_plan(C, C->scratch, P, data, 0, true);
+    enqueue_run(C, C->scratch, P, scale, rdata, false);
+    fetch_results(C, C->scratch, P, res, calc, &st);
+    for (int64_t i = 0; i < n; ++i)
+        if (st[i] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+}
+
+template <class F>
+int guarded(lcb_ctx* C, F&& f) {
+    try {
+        if (C) {
+            std::lock_guard<std::mutex> g(C->mu);
+            set_device(C);
+            f();
+        } else {
+            f();
+        }
+        return LCB_OK;
+    } catch (const Error& e) {
+        if (C) C->last_error = e.what();
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        if (C) C->last_error = "out of host memory";
+        return fail(LCB_ERR_INVALID, "out of host memory");
+    } catch (const std::exception& e) {
+        if (C) C->last_error = e.what();
+        return fail(LCB_ERR_INVALID, e.what());
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* lcb_version(void) { return "lcurve-b200 0.1.0 (sm_100a)"; }
+const char* lcb_last_error(void) { return t_last_error.c_str(); }
+
+int lcb_device_count(int* count) {
+    if (!count) return fail(LCB_ERR_INVALID, "null pointer");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { *count = 0; return fail(LCB_ERR_NO_DEVICE, cudaGetErrorString(e)); }
+    *count = n;
+    return LCB_OK;
+}
+
+int lcb_ctx_create(int device, lcb_ctx** out) {
+    if (!out) return fail(LCB_ERR_INVALID, "null pointer");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return fail(LCB_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n) return fail(LCB_ERR_NO_DEVICE, "device id out of range");
+    auto C = std::make_unique<lcb_ctx>();
+    C->device = device;
+    int rc = guarded(nullptr, [&] {
+        CUDA_TRY(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10) throw Error(LCB_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+        C->num_sms = prop.multiProcessorCount;
+        // fails here, not later, if the sm_100a image cannot load on this device
+        if (lcb::flux_blocks_per_sm() <= 0) throw Error(LCB_ERR_NO_DEVICE, "kernel image not loadable");
+        CUDA_TRY(cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking));
+        C->own_stream = true;
+        for (auto& e : C->ev) CUDA_TRY(cudaEventCreate(&e));
+    });
+    if (rc != LCB_OK) return rc;
+    *out = C.release();
+    return LCB_OK;
+}
+
+void lcb_ctx_destroy(lcb_ctx* C) {
+    if (!C) return;
+    cudaSetDevice(C->device);
+    if (C->stream) cudaStreamSynchronize(C->stream);
+    C->scratch.release();
+    for (auto& e : C->ev)
+        if (e) cudaEventDestroy(e);
+    if (C->own_stream && C->stream) cudaStreamDestroy(C->stream);
+    delete C;
+}
+
+int lcb_ctx_set_stream(lcb_ctx* C, void* stream) {
+    if (!C) return fail(LCB_ERR_INVALID, "null context");
+    return guarded(C, [&] {
+        if (C->own_stream && C->stream) {
+            CUDA_TRY(cudaStreamSynchronize(C->stream));
+            CUDA_TRY(cudaStreamDestroy(C->stream));
+        }
+        C->own_stream = stream == nullptr;
+        if (stream) C->stream = (cudaStream_t)stream;
+        else CUDA_TRY(cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking));
+    });
+}
+
+const char* lcb_ctx_last_error(const lcb_ctx* C) { return C ? C->last_error.c_str() : "null context"; }
+
+// ---- models -----------------------------------------------------------------
+int lcb_model_load(const char* path, lcb_model** out) {
+    if (!path || !out) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] { *out = new lcb_model{lcb::load_model_file(path)}; });
+}
+int lcb_model_parse(const char* text, lcb_model** out) {
+    if (!text || !out) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] { *out = new lcb_model{lcb::parse_model_text(text)}; });
+}
+int lcb_model_clone(const lcb_model* m, lcb_model** out) {
+    if (!m || !out) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] { *out = new lcb_model{m->m}; });
+}
+void lcb_model_destroy(lcb_model* m) { delete m; }
+
+int lcb_model_set_param(lcb_model* m, const char* name, double value) {
+    if (!m || !name) return fail(LCB_ERR_INVALID, "null pointer");
+    int i = lcb::phys_index(name);
+    if (i < 0) return fail(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + name + "'");
+    m->m.p[i].value = value;
+    return LCB_OK;
+}
+int lcb_model_get_param(const lcb_model* m, const char* name, double* value) {
+    if (!m || !name || !value) return fail(LCB_ERR_INVALID, "null pointer");
+    int i = lcb::phys_index(name);
+    if (i < 0) return fail(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + name + "'");
+    *value = m->m.p[i].value;
+    return LCB_OK;
+}
+int lcb_model_get_pparam(const lcb_model* m, const char* name, double* value, double* range, double* dstep,
+                         int* vary, int* defined) {
+    if (!m || !name) return fail(LCB_ERR_INVALID, "null pointer");
+    int i = lcb::phys_index(name);
+    if (i < 0) return fail(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + name + "'");
+    const lcb::Pparam& p = m->m.p[i];
+    if (value) *value = p.value;
+    if (range) *range = p.range;
+    if (dstep) *dstep = p.dstep;
+    if (vary) *vary = p.vary;
+    if (defined) *defined = p.defined;
+    return LCB_OK;
+}
+int lcb_model_set_pparam(lcb_model* m, const char* name, const double* value, const double* range,
+                         const double* dstep, const int* vary) {
+    if (!m || !name) return fail(LCB_ERR_INVALID, "null pointer");
+    int i = lcb::phys_index(name);
+    if (i < 0) return fail(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + name + "'");
+    lcb::Pparam& p = m->m.p[i];
+    if (value) p.value = *value;
+    if (range) p.range = *range;
+    if (dstep) p.dstep = *dstep;
+    if (vary) p.vary = *vary != 0;
+    return LCB_OK;
+}
+int lcb_model_set_comp(lcb_model* m, const char* name, const char* value) {
+    if (!m || !name || !value) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] { lcb::set_comp_param(m->m, name, value); });
+}
+int lcb_model_get_comp(const lcb_model* m, const char* name, char* buf, int buflen) {
+    if (!m || !name || !buf || buflen <= 0) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] {
+        std::string s = lcb::get_comp_param(m->m, name);
+        std::snprintf(buf, (size_t)buflen, "%s", s.c_str());
+    });
+}
+const char* lcb_param_name(int i) { return lcb::phys_name(i); }
+
+// ---- data -------------------------------------------------------------------
+int lcb_read_data(const char* path, lcb_datum** out, int64_t* n) {
+    if (!path || !out || !n) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(nullptr, [&] {
+        std::vector<lcb_datum> d = lcb::read_data_file(path);
+        lcb_datum* p = (lcb_datum*)std::malloc(std::max<size_t>(d.size(), 1) * sizeof(lcb_datum));
+        if (!p) throw std::bad_alloc();
+        if (!d.empty()) std::memcpy(p, d.data(), d.size() * sizeof(lcb_datum));
+        *out = p;
+        *n = (int64_t)d.size();
+    });
+}
+void lcb_free_data(lcb_datum* d) { std::free(d); }
+
+// ---- evaluation ---------------------------------------------------------------
+int lcb_light_curve(lcb_ctx* C, const lcb_model* model, const lcb_datum* data, int64_t n, int scale, int rdata,
+                    double* calc_out, lcb_result* res_out) {
+    if (!C || !model || (!data && n > 0) || !calc_out) return fail(LCB_ERR_INVALID, "null pointer");
+    if (n <= 0) return fail(LCB_ERR_EMPTY, "No data points");
+    return guarded(C, [&] {
+        const lcb::Model* mp = &model->m;
+        int64_t st = 0, cnt = n;
+        std::vector<double> res, calc;
+        std::vector<int> status;
+        lcb::Plan P;
+        run_transient(C, &mp, 1, data, &st, &cnt, scale, rdata, res, &calc, P, status);
+        if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
+        if (status[0] & lcb::kStatusIterCap)
+            throw Error(LCB_ERR_DEVICE_CHECK, "a device-side iteration cap tripped for this model");
+        std::memcpy(calc_out, calc.data(), n * sizeof(double));
+        if (res_out) fill_result(res.data(), res_out);
+    });
+}
+
+int lcb_chisq_batch(lcb_ctx* C, const lcb_model* base, const lcb_datum* data, int64_t n, const char* const* names,
+                    int ndim, const double* values, int64_t nsets, int scale, double* chisq_out) {
+    if (!C || !base || !data || !names || !values || !chisq_out) return fail(LCB_ERR_INVALID, "null pointer");
+    if (ndim <= 0 || nsets < 0) return fail(LCB_ERR_INVALID, "ndim must be > 0");
+    if (n <= 0) return fail(LCB_ERR_EMPTY, "No data points");
+    return guarded(C, [&] {
+        std::vector<int> idx(ndim);
+        for (int j = 0; j < ndim; ++j) idx[j] = lcb::phys_index(names[j]);  // unknown names are ignored
+        std::vector<lcb::Model> ms(nsets, base->m);
+        std::vector<const lcb::Model*> mp(nsets);
+        for (int64_t i = 0; i < nsets; ++i) {
+            for (int j = 0; j < ndim; ++j)
+                if (idx[j] >= 0) ms[i].p[idx[j]].value = values[i * ndim + j];
+            mp[i] = &ms[i];
+        }
+        if (nsets == 0) return;
+        std::vector<int64_t> st(nsets, 0), cnt(nsets, n);
+        std::vector<double> res;
+        std::vector<int> status;
+        lcb::Plan P;
+        run_transient(C, mp.data(), nsets, data, st.data(), cnt.data(), scale, 1, res, nullptr, P, status);
+        for (int64_t i = 0; i < nsets; ++i) chisq_out[i] = P.model_ok[i] ? res[i * 12 + 1] : NAN;
+    });
+}
+
+int lcb_chisq_batch_ragged(lcb_ctx* C, const lcb_model* const* models, int64_t nmodels, const lcb_datum* data,
+                           const int64_t* offsets, int scale, double* chisq_out, double* calc_out,
+                           lcb_result* res_out) {
+    if (!C || !models || !data || !offsets || !chisq_out) return fail(LCB_ERR_INVALID, "null pointer");
+    if (nmodels <= 0) return fail(LCB_ERR_INVALID, "nmodels must be > 0");
+    return guarded(C, [&] {
+        std::vector<const lcb::Model*> mp(nmodels);
+        std::vector<int64_t> st(nmodels), cnt(nmodels);
+        for (int64_t i = 0; i < nmodels; ++i) {
+            if (!models[i]) throw Error(LCB_ERR_INVALID, "null model");
+            mp[i] = &models[i]->m;
+            st[i] = offsets[i];
+            cnt[i] = offsets[i + 1] - offsets[i];
+            if (cnt[i] < 0) throw Error(LCB_ERR_INVALID, "offsets must be non-decreasing");
+        }
+        std::vector<double> res, calc;
+        std::vector<int> status;
+        lcb::Plan P;
+        run_transient(C, mp.data(), nmodels, data, st.data(), cnt.data(), scale, 1, res, calc_out ? &calc : nullptr, P,
+                      status);
+        for (int64_t i = 0; i < nmodels; ++i) {
+            chisq_out[i] = P.model_ok[i] ? res[i * 12 + 1] : NAN;
+            if (res_out) {
+                if (P.model_ok[i]) fill_result(&res[i * 12], &res_out[i]);
+                else {
+                    double nanv[12];
+                    for (double& v : nanv) v = NAN;
+                    fill_result(nanv, &res_out[i]);
+                }
+            }
+        }
+        if (calc_out)
+            for (int64_t d = 0; d < P.ndatum; ++d) calc_out[offsets[0] + d] = calc[d];
+    });
+}
+
+// ---- resident batch -------------------------------------------------------------
+int lcb_batch_create(lcb_ctx* C, const lcb_model* const* models, int64_t nmodels, const lcb_datum* data,
+                     const int64_t* offsets, lcb_batch** out) {
+    if (!C || !models || !data || !offsets || !out) return fail(LCB_ERR_INVALID, "null pointer");
+    if (nmodels <= 0) return fail(LCB_ERR_INVALID, "nmodels must be > 0");
+    *out = nullptr;
+    auto B = std::make_unique<lcb_batch>();
+    B->ctx = C;
+    int rc = guarded(C, [&] {
+        int64_t total = offsets[nmodels] - offsets[0];
+        if (total < 0) throw Error(LCB_ERR_INVALID, "offsets must be non-decreasing");
+        B->data.assign(data + offsets[0], data + offsets[0] + total);
+        for (int64_t i = 0; i < nmodels; ++i) {
+            if (!models[i]) throw Error(LCB_ERR_INVALID, "null model");
+            check_iscale(models[i]->m);
+            B->models.push_back(models[i]->m);
+            B->start.push_back(offsets[i] - offsets[0]);
+            B->count.push_back(offsets[i + 1] - offsets[i]);
+            if (B->count.back() < 0) throw Error(LCB_ERR_INVALID, "offsets must be non-decreasing");
+        }
+        std::vector<const lcb::Model*> mp(nmodels);
+        for (int64_t i = 0; i < nmodels; ++i) mp[i] = &B->models[i];
+        lcb::plan_batch(mp.data(), nmodels, B->data.data(), B->start.data(), B->count.data(), C->num_sms, B->plan);
+        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), true);
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+    });
+    if (rc != LCB_OK) {
+        B->dev.release();
+        return rc;
+    }
+    *out = B.release();
+    return LCB_OK;
+}
+
+void lcb_batch_destroy(lcb_batch* B) {
+    if (!B) return;
+    std::lock_guard<std::mutex> g(B->ctx->mu);
+    cudaSetDevice(B->ctx->device);
+    cudaStreamSynchronize(B->ctx->stream);
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->dev.release();
+    delete B;
+}
+
+int lcb_batch_set_params(lcb_batch* B, const char* const* names, int ndim, const double* values) {
+    if (!B || !names || !values || ndim <= 0) return fail(LCB_ERR_INVALID, "bad arguments");
+    lcb_ctx* C = B->ctx;
+    return guarded(C, [&] {
+        const int64_t n = (int64_t)B->models.size();
+        for (int j = 0; j < ndim; ++j) {
+            int k = lcb::phys_index(names[j]);
+            if (k < 0) throw Error(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + names[j] + "'");
+            for (int64_t i = 0; i < n; ++i) B->models[i].p[k].value = values[i * ndim + j];
+        }
+        std::vector<const lcb::Model*> mp(n);
+        for (int64_t i = 0; i < n; ++i) mp[i] = &B->models[i];
+        lcb::Plan P;
+        lcb::plan_batch(mp.data(), n, B->data.data(), B->start.data(), B->count.data(), C->num_sms, P);
+        bool same = P.shape_key == B->plan.shape_key;
+        B->plan = std::move(P);
+        // unchanged shapes: only the model table and the tables derived from it change
+        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
+        if (!same && B->graph) {
+            cudaGraphExecDestroy(B->graph);
+            B->graph = nullptr;
+        }
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+    });
+}
+
+int lcb_batch_run(lcb_batch* B, int scale) {
+    if (!B) return fail(LCB_ERR_INVALID, "null batch");
+    lcb_ctx* C = B->ctx;
+    return guarded(C, [&] {
+        if (B->graph && (B->graph_scale != scale || B->graph_key != B->plan.shape_key)) {
+            cudaGraphExecDestroy(B->graph);
+            B->graph = nullptr;
+        }
+        if (!B->graph) {
+            // the flux kernel's shared-memory attribute must be set outside capture
+            lcb::flux_blocks_per_sm();
+            cudaGraph_t g;
+            CUDA_TRY(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_run(C, B->dev, B->plan, scale, 1, true);
+            } catch (...) {
+                cudaStreamEndCapture(C->stream, &g);
+                throw;
+            }
+            CUDA_TRY(cudaStreamEndCapture(C->stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&B->graph, g, 0);
+            cudaGraphDestroy(g);
+            CUDA_TRY(e);
+            B->graph_scale = scale;
+            B->graph_key = B->plan.shape_key;
+        }
+        CUDA_TRY(cudaGraphLaunch(B->graph, C->stream));
+        fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
+        for (int k = 0; k < 4; ++k) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, C->ev[k], C->ev[k + 1]) == cudaSuccess) B->stage_ms[k] = ms;
+        }
+        B->ran = true;
+        for (int s : B->h_status)
+            if (s & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+    });
+}
+
+int lcb_batch_results(lcb_batch* B, double* chisq_out, double* calc_out, lcb_result* res_out) {
+    if (!B) return fail(LCB_ERR_INVALID, "null batch");
+    if (!B->ran) return fail(LCB_ERR_INVALID, "lcb_batch_run has not been called");
+    lcb_ctx* C = B->ctx;
+    return guarded(C, [&] {
+        const lcb::Plan& P = B->plan;
+        const int64_t n = (int64_t)P.models.size();
+        for (int64_t i = 0; i < n; ++i) {
+            if (chisq_out) chisq_out[i] = P.model_ok[i] ? B->h_results[i * 12 + 1] : NAN;
+            if (res_out) {
+                double nanv[12];
+                for (double& v : nanv) v = NAN;
+                fill_result(P.model_ok[i] ? &B->h_results[i * 12] : nanv, &res_out[i]);
+            }
+        }
+        if (calc_out && P.ndatum) {
+            CUDA_TRY(cudaMemcpy(calc_out, B->dev.calc.p, P.ndatum * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+    });
+}
+
+int lcb_batch_stats(const lcb_batch* B, int64_t* out8) {
+    if (!B || !out8) return fail(LCB_ERR_INVALID, "null pointer");
+    const lcb::Plan& P = B->plan;
+    int64_t v[8] = {(int64_t)P.models.size(), P.nelem, P.nsub, P.evals, (int64_t)P.units.size(), P.roche_elems, 0, 0};
+    std::memcpy(out8, v, sizeof v);
+    return LCB_OK;
+}
+
+int lcb_batch_stage_ms(const lcb_batch* B, double* out4) {
+    if (!B || !out4) return fail(LCB_ERR_INVALID, "null pointer");
+    for (int k = 0; k < 4; ++k) out4[k] = B->stage_ms[k];
+    return LCB_OK;
+}
+
+}  // extern "C"

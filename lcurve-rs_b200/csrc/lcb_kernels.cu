@@ -1,0 +1,1240 @@
+// lcb_kernels.cu — sm_100a kernels of the light-curve path.
+//
+//   k_elements : one thread per grid element of every model in the batch.
+//                Surface point (surface.rs:54-121) or sphere point, area,
+//                gravity (grid.rs:201-322; disc/rim/spot grid.rs:336-553);
+//                eclipse intervals by the other star -- FP64 Roche ray-march
+//                ingress_egress (eclipse.rs:270-373) or the analytic sphere
+//                case (eclipse.rs:229-265) -- and by an opaque disc
+//                (disc_eclipse.rs:84-330); continuum flux (brightness.rs);
+//                per-model FP64 reductions for ginterp, wdwarf, log g, radii.
+//   k_phase    : one thread per datum: ephemeris + Roemer phase and the
+//                exposure sub-divisions (orchestration.rs:231-241,
+//                flux.rs:379-387) with their earth vectors.
+//   k_flux     : persistent FP32 flux sum (flux.rs:7-111) over work units of
+//                (element range x 512 sub-phases).  Element chunks arrive in
+//                shared memory by cp.async.bulk (TMA) double buffering; each
+//                thread keeps 4 sub-phases in registers and accumulates in
+//                FP32 blocks of 32 elements folded into a two-sum pair.
+//                Visibility is decided exactly in FP64 per (element, tile)
+//                and per sub-phase only where an eclipse edge falls inside
+//                the tile.
+//   k_epilogue : one block per model: ginterp scale factors, exposure
+//                smearing, slope/third, chi-squared / re_scale
+//                (orchestration.rs:243-310, 361-401).
+#include <cfloat>
+#include <cstdint>
+
+#include "lcb_kernels.cuh"
+
+namespace lcb {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2.0 * kPi;
+constexpr double kFac1 = 2.0e27 * 6.6262e-34 * 2.99792458e8;      // planck.rs:5
+constexpr double kFac2 = 1.0e9 * 6.6262e-34 * 2.99792458e8 / 1.3806e-23;  // planck.rs:8
+constexpr double kFwhmEfac = 2.3548200450309493;                  // brightness.rs:8
+constexpr double kEfac = 1.0000001;                               // grid.rs:396
+constexpr int kFblinkEvalCap = 1 << 18;  // bound on one line-of-sight search (reference has none)
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+__device__ __forceinline__ double rad2deg(double r) { return r * (180.0 / kPi); }
+
+__device__ __forceinline__ double planck_d(double wave, double temp) {  // planck.rs:16-23
+    double e = kFac2 / (wave * temp);
+    if (e > 40.0) return kFac1 * exp(-e) / (wave * sq(wave));
+    return kFac1 / (exp(e) - 1.0) / (wave * sq(wave));
+}
+
+// ---------------------------------------------------------------------------
+// Roche potentials
+// ---------------------------------------------------------------------------
+// Exact-rounding potential (surface.rs:54-121 builds the stars from it).
+__device__ __forceinline__ double pot_exact(bool primary, double q, double ssq, double x, double y, double z) {
+    double mu = q / (1.0 + q), comp = 1.0 - mu;
+    double x2y2 = sq(x) + sq(y);
+    double r1sq = x2y2 + sq(z);
+    double r1 = sqrt(r1sq), r2 = sqrt(r1sq + 1.0 - 2.0 * x);
+    if (primary) return -comp / r1 - mu / r2 - ssq * x2y2 / 2.0 + mu * x;
+    return -comp / r1 - mu / r2 - ssq * (0.5 + 0.5 * x2y2 - x) - comp * x;
+}
+__device__ __forceinline__ void dpot_exact(bool primary, double q, double ssq, double x, double y, double z,
+                                           double& gx, double& gy, double& gz) {
+    double r1sq = x * x + y * y + z * z, r2sq = r1sq + 1.0 - 2.0 * x;
+    double r1 = sqrt(r1sq), r2 = sqrt(r2sq);
+    double mu = q / (1.0 + q);
+    double mu1 = mu / r2 / r2sq, comp = (1.0 - mu) / r1 / r1sq;
+    gx = comp * x + mu1 * (x - 1.0) - (primary ? ssq * x - mu : ssq * (x - 1.0) - mu + 1.0);
+    gy = comp * y + mu1 * y - ssq * y;
+    gz = comp * z + mu1 * z;
+}
+
+// Potential along a line of sight p + lam*e for the eclipse search
+// (potential.rs:110-117).  1/r from rsqrt: decisions against pref differ
+// from the divided form only within an ulp of the surface.
+struct Los {
+    double px, py, pz, ex, ey, ez;
+};
+__device__ __forceinline__ double los_pot(const RocheEcl& s, const Los& L, double lam) {
+    double x = fma(lam, L.ex, L.px), y = fma(lam, L.ey, L.py), z = fma(lam, L.ez, L.pz);
+    double x2y2 = x * x + y * y;
+    double r1sq = x2y2 + z * z;
+    double r2sq = r1sq + 1.0 - 2.0 * x;
+    double v = -s.comp * rsqrt(r1sq) - s.mu * rsqrt(r2sq);
+    if (s.primary) return v - s.ssq * x2y2 * 0.5 + s.mu * x;
+    return v - s.ssq * (0.5 + 0.5 * x2y2 - x) - s.comp * x;
+}
+__device__ __forceinline__ double los_dpot(const RocheEcl& s, const Los& L, double lam) {  // potential.rs:120-127
+    double x = fma(lam, L.ex, L.px), y = fma(lam, L.ey, L.py), z = fma(lam, L.ez, L.pz);
+    double r1sq = x * x + y * y + z * z, r2sq = r1sq + 1.0 - 2.0 * x;
+    double i1 = rsqrt(r1sq), i2 = rsqrt(r2sq);
+    double comp = s.comp * (i1 * i1 * i1), mu1 = s.mu * (i2 * i2 * i2);
+    double gx = comp * x + mu1 * (x - 1.0) - (s.primary ? s.ssq * x - s.mu : s.ssq * (x - 1.0) - s.mu + 1.0);
+    double gy = comp * y + mu1 * y - s.ssq * y;
+    double gz = comp * z + mu1 * z;
+    return gx * L.ex + gy * L.ey + gz * L.ez;
+}
+
+// dbrent with stop-fast (crates/subs/src/numerical/dbrent.rs:20-165).
+// Returns 1 = bracketed minimum below fref, 0 = not below, and uses *evals.
+__device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double bx, double cx, double acc,
+                             double fref, int& evals) {
+    double a = fmin(ax, cx), b = fmax(ax, cx);
+    double x = bx, w = bx, v = bx;
+    double fx = los_pot(s, L, x), fw = fx, fv = fx;
+    ++evals;
+    if (fx < fref) return true;
+    double dx = los_dpot(s, L, x), dw = dx, dv = dx;
+    double e = 0.0, d = 0.0;
+    for (int it = 0; it < 100; ++it) {
+        double xm = 0.5 * (a + b);
+        double tol1 = acc, tol2 = 2.0 * tol1;
+        if (fabs(x - xm) <= tol2 - 0.5 * (b - a)) return fx < fref;
+        if (fabs(e) > tol1) {
+            double d1 = 2.0 * (b - a), d2 = d1;
+            if (dw != dx) d1 = (w - x) * dx / (dx - dw);
+            if (dv != dx) d2 = (v - x) * dx / (dx - dv);
+            double u1 = x + d1, u2 = x + d2;
+            bool ok1 = (a - u1) * (u1 - b) > 0.0 && dx * d1 <= 0.0;
+            bool ok2 = (a - u2) * (u2 - b) > 0.0 && dx * d2 <= 0.0;
+            double olde = e;
+            e = d;
+            if (ok1 || ok2) {
+                d = (ok1 && ok2) ? (fabs(d1) < fabs(d2) ? d1 : d2) : (ok1 ? d1 : d2);
+                if (fabs(d) <= fabs(0.5 * olde)) {
+                    double u = x + d;
+                    if (u - a < tol2 || b - u < tol2) d = (xm - x >= 0.0) ? fabs(tol1) : -fabs(tol1);
+                } else {
+                    e = dx >= 0.0 ? a - x : b - x;
+                    d = 0.5 * e;
+                }
+            } else {
+                e = dx >= 0.0 ? a - x : b - x;
+                d = 0.5 * e;
+            }
+        } else {
+            e = dx >= 0.0 ? a - x : b - x;
+            d = 0.5 * e;
+        }
+        double u, fu;
+        if (fabs(d) >= tol1) {
+            u = x + d;
+            fu = los_pot(s, L, u);
+            ++evals;
+            if (fu < fref) return true;
+        } else {
+            u = x + (d >= 0.0 ? fabs(tol1) : -fabs(tol1));
+            fu = los_pot(s, L, u);
+            ++evals;
+            if (fu < fref) return true;
+            if (fu > fx) return fx < fref;
+        }
+        double du = los_dpot(s, L, u);
+        if (fu <= fx) {
+            if (u >= x) a = x; else b = x;
+            v = w; fv = fw; dv = dw;
+            w = x; fw = fx; dw = dx;
+            x = u; fx = fu; dx = du;
+        } else {
+            if (u < x) a = u; else b = u;
+            if (fu <= fw || w == x) {
+                v = w; fv = fw; dv = dw;
+                w = u; fw = fu; dw = du;
+            } else if (fu < fv || v == x || v == w) {
+                v = u; fv = fu; dv = du;
+            }
+        }
+    }
+    return false;  // iteration cap: the reference maps its Err to "not eclipsed"
+}
+
+// Is point p hidden from earth direction e by the Roche star? (eclipse.rs:123-197)
+__device__ bool fblink(const RocheEcl& s, double acc, const Los& L, int& evals, bool& capped) {
+    double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
+    double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
+    if (bq >= 0.0) return false;
+    double cq = (dx * dx + dy * dy + dz * dz) - sq(s.rref);
+    double fac = sq(bq) - cq;
+    if (fac <= 0.0) return false;
+    fac = sqrt(fac);
+    double lam2 = -bq + fac, lam1 = fmax(cq / lam2, 0.0);
+    if (lam1 == 0.0) return true;
+    const double pref = s.pref;
+    int nstep = 1;
+    double step = lam2 - lam1, f1 = 0.0, f2 = 0.0, flam = 1.0, lam = lam1;
+    int local = 0;
+    while (step > acc) {
+        lam = lam1 + step / 2.0;
+        bool br = false;
+        for (int n = 0; n < nstep; ++n) {
+            flam = los_pot(s, L, lam + (double)n * step);
+            ++local;
+            if (flam <= pref) { evals += local; return true; }
+            if (nstep == 1) { f1 = los_pot(s, L, lam1); f2 = los_pot(s, L, lam2); local += 2; }
+            if (flam < f1 && flam < f2) { lam = lam + (double)n * step; br = true; break; }
+        }
+        if (br) break;
+        if (local > kFblinkEvalCap) { capped = true; evals += local; return false; }
+        step /= 2.0;
+        nstep *= 2;
+    }
+    evals += local;
+    if (flam < f1 && flam < f2) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, evals);
+    return false;
+}
+
+__device__ __forceinline__ void earth_at(double cosi, double sini, double phase, double& ex, double& ey, double& ez) {
+    double sn, cs;  // misc.rs:42-45
+    sincos(kTwoPi * phase, &sn, &cs);
+    ex = sini * cs;
+    ey = -sini * sn;
+    ez = cosi;
+}
+
+// Analytic sphere eclipse (eclipse.rs:229-265).
+__device__ bool sphere_phase(double cosi, double sini, double px, double py, double pz, double cx, double rs,
+                             double& phi1, double& phi2, double& lam1, double& lam2) {
+    double dx = px - cx, dy = py, dz = pz;
+    double pdist = sqrt(sq(dx) + sq(dy));
+    double bq = dz * cosi - pdist * sini;
+    if (bq >= 0.0) return false;
+    double cq = (dx * dx + dy * dy + dz * dz) - sq(rs);
+    double fac = sq(bq) - cq;
+    if (fac <= 0.0) return false;
+    fac = sqrt(fac);
+    lam2 = -bq + fac;
+    lam1 = fmax(cq / lam2, 0.0);
+    if (cq < 0.0) {
+        phi1 = 0.0;
+        phi2 = 1.0;
+    } else {
+        double delta = acos((cosi * dz + sqrt(cq)) / (sini * pdist));
+        double phi = atan2(dy, -dx);
+        double p1 = (phi - delta) / kTwoPi;
+        p1 -= floor(p1);
+        phi1 = p1;
+        phi2 = p1 + 2.0 * delta / kTwoPi;
+    }
+    return true;
+}
+
+// Ingress/egress of point p behind a Roche-distorted star (eclipse.rs:270-373).
+__device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
+                               double pz, double& ing, double& eg, bool& capped) {
+    double phi1, phi2, lam1, lam2;
+    if (!sphere_phase(cosi, sini, px, py, pz, s.cofmx, s.rref, phi1, phi2, lam1, lam2)) return false;
+    double acc = 2.0 * sqrt(2.0 * kTwoPi * (lam2 - lam1) * delta);
+    Los L{px, py, pz, 0.0, 0.0, 0.0};
+    int evals = 0;
+    // pot_min_search: first scanned phase that is eclipsed (eclipse.rs:347-373)
+    double ns = ceil((phi2 - phi1) / (acc / kTwoPi));
+    int nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
+    double dphi = (phi2 - phi1) / (double)nsteps;
+    double phi = 0.0;
+    bool found = false;
+    for (int i = 0; i <= nsteps; ++i) {
+        phi = phi1 + (double)i * dphi;
+        earth_at(cosi, sini, phi, L.ex, L.ey, L.ez);
+        if (fblink(s, acc, L, evals, capped)) { found = true; break; }
+        if (capped) return false;
+    }
+    if (!found) return false;
+    auto chop = [&](double pin, double pout) {
+        for (int it = 0; it < 200 && fabs(pin - pout) > delta; ++it) {
+            double pmid = (pin + pout) / 2.0;
+            earth_at(cosi, sini, pmid, L.ex, L.ey, L.ez);
+            if (fblink(s, acc, L, evals, capped)) pin = pmid; else pout = pmid;
+        }
+        return (pin + pout) / 2.0;
+    };
+    ing = chop(phi, phi1);
+    ing -= floor(ing);
+    eg = chop(phi, phi2);
+    eg -= floor(eg);
+    if (eg < ing) eg += 1.0;
+    return true;
+}
+
+// Disc occultation (disc_eclipse.rs:29-70, 84-330); returns the number of pairs (<= 2).
+__device__ __forceinline__ double cut_phase(double rxy, double rcone, double radius) {
+    double c = (sq(rxy) + sq(rcone) - sq(radius)) / (2.0 * rcone * rxy);
+    return acos(fmin(fmax(c, -1.0), 1.0)) / kTwoPi;
+}
+enum { C_ABOVE, C_INSIDE, C_OUTSIDE, C_SEPARATE, C_CROSSING };
+__device__ __forceinline__ int circle_ecl(double rxy, double z, double zc, double radius, double tani, double& ph) {
+    ph = 0.0;
+    if (z >= zc) return C_ABOVE;
+    double rcone = tani * (zc - z);
+    if (rcone >= rxy + radius) return C_OUTSIDE;
+    if (rxy >= rcone + radius) return C_SEPARATE;
+    if (rxy + rcone <= radius) return C_INSIDE;
+    ph = cut_phase(rxy, rcone, radius);
+    return C_CROSSING;
+}
+__device__ int disc_eclipse(const ModelDev& M, double rdisc1, double px, double py, double pz, double* ing,
+                            double* eg) {
+    const double rdisc2 = M.rdisc2, beta = M.beta, height = M.height;
+    double hout = height * pow(rdisc2, beta);
+    if (pz >= hout) return 0;
+    double sini = M.sini_d, cosi = M.cosi_d;
+    if (cosi == 0.0) {
+        if (fabs(pz) < hout) {
+            double rxy = sqrt(sq(px) + sq(py));
+            if (rxy <= rdisc2) { ing[0] = 0.0; eg[0] = 1.0; return 1; }
+            double subtend = asin(rdisc2 / rxy) / kTwoPi;
+            double pc = atan2(py, -px) / kTwoPi;
+            double i0 = pc - subtend;
+            i0 -= floor(i0);
+            ing[0] = i0; eg[0] = i0 + 2.0 * subtend;
+            return 1;
+        }
+        return 0;
+    }
+    double rxy = sqrt(sq(px) + sq(py));
+    if (rdisc1 < rxy && rxy < rdisc2 && fabs(pz) < height * pow(rxy, beta)) { ing[0] = 0.0; eg[0] = 1.1; return 1; }
+    double tani = sini / cosi;
+    if (rxy < rdisc2 && pz >= height * pow(fmax(rdisc1, rxy), beta)) {
+        double ph;
+        int r = circle_ecl(rxy, pz, hout, rdisc2, tani, ph);
+        if (r == C_OUTSIDE) { ing[0] = 0.0; eg[0] = 1.1; return 1; }
+        if (r == C_CROSSING) {
+            double i0 = atan2(py, -px) / kTwoPi + ph;
+            i0 -= floor(i0);
+            ing[0] = i0; eg[0] = i0 + 1.0 - 2.0 * ph;
+            return 1;
+        }
+        return 0;
+    }
+    double rlo = fmax(tani * (-hout - pz), 0.0);
+    if (rlo >= rxy + rdisc2) return 0;
+    double rhi = tani * (hout - pz);
+    if (rxy >= rhi + rdisc2) return 0;
+    double ecl;
+    if (rxy + rlo <= rdisc2) ecl = 0.5;
+    else if (rxy <= rdisc2) ecl = cut_phase(rxy, rlo, rdisc2);
+    else if (sq(rhi) + sq(rdisc2) >= sq(rxy) && sq(rlo) + sq(rdisc2) <= sq(rxy)) ecl = asin(rdisc2 / rxy) / kTwoPi;
+    else if (sq(rhi) + sq(rdisc2) < sq(rxy)) ecl = cut_phase(rxy, rhi, rdisc2);
+    else ecl = cut_phase(rxy, rlo, rdisc2);
+    double hin = height * pow(rdisc1, beta);
+    double app = -1.0;
+    auto first = [&](double zc, double rad) {
+        double ph;
+        int r = circle_ecl(rxy, pz, zc, rad, tani, ph);
+        if (r == C_INSIDE) app = 0.5; else if (r == C_CROSSING) app = ph;
+    };
+    auto next = [&](double zc, double rad) {
+        if (!(app > 0.0)) return;
+        double ph;
+        int r = circle_ecl(rxy, pz, zc, rad, tani, ph);
+        if (r == C_CROSSING) app = fmin(app, ph); else if (r != C_INSIDE) app = -1.0;
+    };
+    if (pz < -hout) {
+        first(-hout, rdisc2); next(-hin, rdisc1); next(hin, rdisc1); next(hout, rdisc2);
+    } else if (rxy < rdisc1) {
+        if (pz < -hin) { first(-hin, rdisc1); next(hin, rdisc1); next(hout, rdisc2); }
+        else if (pz < hin) { first(hin, rdisc1); next(hout, rdisc2); }
+    }
+    double phi0 = atan2(py, -px) / kTwoPi;
+    if (app <= 0.0) {
+        double i0 = phi0 - ecl;
+        i0 -= floor(i0);
+        ing[0] = i0; eg[0] = i0 + 2.0 * ecl;
+        return 1;
+    }
+    if (app < ecl) {
+        double i0 = phi0 - ecl;
+        i0 -= floor(i0);
+        ing[0] = i0; eg[0] = i0 + (ecl - app);
+        double i1 = phi0 + app;
+        i1 -= floor(i1);
+        ing[1] = i1; eg[1] = i1 + (ecl - app);
+        return 2;
+    }
+    return 0;
+}
+
+// Irradiated temperature (brightness.rs:150-174) -> temp, geom.
+__device__ __forceinline__ double irradiate(double tbase, double gravity, double gdcbol, double absorb, double tirr,
+                                            double mu, double r, double rirr, double& geom) {
+    double tg = tbase * pow(gravity, gdcbol);
+    double tg4 = sq(tg) * sq(tg), ti4 = sq(tirr) * sq(tirr);
+    if (mu >= rirr) {
+        geom = sq(rirr / r) * mu;
+        return pow(tg4 + absorb * ti4 * geom, 0.25);
+    }
+    if (mu > -rirr) {
+        double x0 = -mu / rirr;
+        geom = sq(rirr / r) * rirr * (sqrt(1.0 - x0 * x0) * (2.0 + x0 * x0) / 3.0 - x0 * (kPi / 2.0 - asin(x0))) / kPi;
+        return pow(tg4 + absorb * ti4 * geom, 0.25);
+    }
+    geom = 0.0;
+    return tg;
+}
+
+__device__ __forceinline__ double ang_dist(double px, double py, double pz, const SpotDev& s, double len) {
+    if (len <= 0.0) return 180.0;  // brightness.rs:177-183
+    double c = fmin(fmax((px * s.dx + py * s.dy + pz * s.dz) / len, -1.0), 1.0);
+    return rad2deg(acos(c));
+}
+
+// LDC::imu in FP64 (types.rs:101-119)
+__device__ __forceinline__ double imu_d(const double* l, int ltype, double mu) {
+    if (mu <= 0.0) return 0.0;
+    mu = fmin(mu, 1.0);
+    double om = 1.0 - mu, im = 1.0;
+    if (ltype == 0) {
+        im -= om * (l[0] + om * (l[1] + om * (l[2] + om * l[3])));
+    } else {
+        im -= l[0] + l[1] + l[2] + l[3];
+        double ms = sqrt(mu);
+        im += ms * (l[0] + ms * (l[1] + ms * (l[2] + ms * l[3])));
+    }
+    return im;
+}
+
+__device__ __forceinline__ double lens_mag_d(double sx, double sy, double sz, double ex, double ey, double ez,
+                                             double rl) {  // flux.rs:390-406
+    double d = -(sx * ex + sy * ey + sz * ez);
+    if (d <= 0.0) return 1.0;
+    double ax = sx + d * ex, ay = sy + d * ey, az = sz + d * ez;
+    double p = sqrt(ax * ax + ay * ay + az * az), ph = p / 2.0, phsq = ph * ph, rd = rl * d;
+    double pd = phsq > 25.0 * rd ? p + rd / p : ph + sqrt(phsq + rd);
+    return pd * pd / (pd - ph) / ph / 4.0;
+}
+
+// ---------------------------------------------------------------------------
+// k_elements
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
+    const ElemBlock blk = A.blocks[blockIdx.x];
+    const SegDesc sg = A.segs[blk.seg];
+    const ModelDev& M = A.models[sg.model];
+    const int64_t i = blk.offset + threadIdx.x;
+    const bool valid = i < sg.count;
+
+    double px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 1;
+    float area = 0.f, grav = 1.f, flux = 0.f;
+    double ing[kMaxEcl], eg[kMaxEcl];
+    int necl = 0, nse = 0;  // total pairs; pairs from the star eclipse (before disc pairs)
+    bool capped = false;
+
+    auto star_ecl = [&](int by, double x, double y, double z) {  // grid.rs:49-73
+        const bool roche = by == 1 ? M.roche1 : M.roche2;
+        double a, b;
+        if (roche) {
+            if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, x, y, z, a, b, capped)) {
+                ing[necl] = a; eg[necl] = b; ++necl;
+            }
+        } else {
+            double l1, l2;
+            if (sphere_phase(M.cosi_e, M.sini_e, x, y, z, by == 1 ? 0.0 : 1.0, by == 1 ? M.r1 : M.r2, a, b, l1, l2)) {
+                ing[necl] = a; eg[necl] = b; ++necl;
+            }
+        }
+    };
+
+    if (valid) {
+        if (sg.kind == SEG_STAR1 || sg.kind == SEG_STAR2) {
+            const bool primary = sg.kind == SEG_STAR1;
+            // band of element i (grid.rs:227-262)
+            int lo = 0, hi = sg.ntable - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (A.bands[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
+            }
+            const Band b = A.bands[sg.table + lo];
+            const int64_t np = i - b.first;
+            double phi = b.phi1 + (b.phi2 - b.phi1) * ((double)np + 0.5) / (double)b.nphi;
+            double sinp, cosp;
+            sincos(phi, &sinp, &cosp);
+            double ux, uy, uz;
+            if (M.npole) { ux = b.sint * cosp; uy = b.sint * sinp; uz = b.cost; }
+            else { ux = b.cost; uy = b.sint * cosp; uz = b.sint * sinp; }
+            const bool roche = primary ? M.roche1 : M.roche2;
+            const double cofm = primary ? 0.0 : 1.0;
+            double rad, g;
+            if (roche) {  // face (surface.rs:54-121)
+                const double ssq = primary ? sq(M.spin1) : sq(M.spin2);
+                const double rref = primary ? M.rref1 : M.rref2, pref = primary ? M.pref1 : M.pref2;
+                double rlo = rref / 2.0, rhi = rref, t = pref + 1.0;
+                for (int k = 0; k < 30 && t > pref; ++k) {
+                    rlo = rhi / 2.0;
+                    t = pot_exact(primary, M.q, ssq, cofm + rlo * ux, rlo * uy, rlo * uz);
+                    if (t > pref) rhi = rlo;
+                }
+                for (int k = 0; k < 100 && rhi - rlo > M.acc_face; ++k) {
+                    double mid = (rlo + rhi) / 2.0;
+                    if (pot_exact(primary, M.q, ssq, cofm + mid * ux, mid * uy, mid * uz) < pref) rlo = mid;
+                    else rhi = mid;
+                }
+                rad = (rlo + rhi) / 2.0;
+                px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
+                double gx, gy, gz;
+                dpot_exact(primary, M.q, ssq, px, py, pz, gx, gy, gz);
+                g = sqrt(gx * gx + gy * gy + gz * gz);
+                double n2 = gx * gx + gy * gy + gz * gz;
+                if (n2 > 0.0) { double nn = sqrt(n2); dx = gx / nn; dy = gy / nn; dz = gz / nn; }
+                else { dx = gx; dy = gy; dz = gz; }
+            } else {
+                rad = primary ? M.r1 : M.r2;
+                px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
+                dx = ux; dy = uy; dz = uz;
+                g = 1.0;
+            }
+            area = (float)(((b.aphi * rad) * b.sint) * (b.ath * rad) / (ux * dx + uy * dy + uz * dz));
+            grav = (float)(g / (primary ? M.gref1 : M.gref2));
+            if (primary ? M.eclipse1 : M.eclipse2) star_ecl(primary ? 2 : 1, px, py, pz);
+            nse = necl;
+            if (M.add_disc && M.opaque)  // orchestration.rs:145-157
+                necl += disc_eclipse(M, M.rdisc1_l, px, py, pz, ing + necl, eg + necl);
+            // continuum (brightness.rs:49-144)
+            const double cx = primary ? 1.0 : 0.0;
+            double vx = cx - px, vy = -py, vz = -pz;
+            double r = sqrt(vx * vx + vy * vy + vz * vz);
+            double mu = (dx * vx + dy * vy + dz * vz) / r;
+            double geom, temp;
+            if (primary) {
+                double t1 = M.t1, plen = sqrt(px * px + py * py + pz * pz);
+                for (int k = 0; k < 3; ++k) {
+                    const SpotDev& s = M.spot1[k];
+                    if (!s.on) continue;
+                    double dist = ang_dist(px, py, pz, s, plen);
+                    t1 += (s.tcen - M.t1) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
+                }
+                if (M.uesp_on) {
+                    double el = sqrt(px * px + py * py);
+                    if (el > 0.0) {
+                        double clat = fmin(fmax((px * px + py * py) / el / plen, -1.0), 1.0);
+                        double dlat = rad2deg(acos(clat));
+                        double clong = fmin(fmax((M.uesp_dx * px + M.uesp_dy * py) / el, -1.0), 1.0);
+                        double dlong = rad2deg(acos(clong));
+                        double hw = M.uesp_lathw, lw = M.uesp_longhw, tp = M.uesp_taper, ut = M.uesp_temp;
+                        if (dlat <= hw && dlong <= lw) t1 = ut;
+                        else if (dlat <= hw) t1 += (ut - M.t1) * exp(-(dlong - lw) / tp);
+                        else if (dlong <= lw) t1 += (ut - M.t1) * exp(-(dlat - hw) / tp);
+                        else t1 += (ut - M.t1) * exp(-(dlat - hw) / tp) * exp(-(dlong - lw) / tp);
+                    }
+                }
+                temp = irradiate(t1, (double)grav, M.gdcbol1, M.absorb, M.t2, mu, r, M.r2c, geom);
+                flux = (float)((double)area * planck_d(M.wavelength, temp));
+                if (M.mirror) flux += (float)((double)area * geom * M.planck_t2abs);
+            } else {
+                double t2 = fabs(M.t2);
+                for (int k = 0; k < 2; ++k) {
+                    const SpotDev& s = M.spot2[k];
+                    if (!s.on) continue;
+                    double ox = px - 1.0, oy = py, oz = pz;
+                    double dist = ang_dist(ox, oy, oz, s, sqrt(ox * ox + oy * oy + oz * oz));
+                    t2 += (s.tcen - t2) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
+                }
+                temp = irradiate(t2, (double)grav, M.gdcbol2, M.absorb, M.t1, mu, r, M.r1c, geom);
+                flux = (float)((double)area * planck_d(M.wavelength, temp));
+                if (M.mirror) flux += (float)((double)area * geom * M.planck_t1);
+            }
+        } else if (sg.kind == SEG_DISC) {  // grid.rs:356-390, brightness.rs:204-212
+            int lo = 0, hi = sg.ntable - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (A.rings[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
+            }
+            const Ring g = A.rings[sg.table + lo];
+            double th = kTwoPi * (double)(i - g.first) / (double)g.ntheta;
+            double st, ct;
+            sincos(th, &st, &ct);
+            px = g.rad * ct; py = g.rad * st; pz = g.h;
+            dx = -ct * g.sinp; dy = -st * g.sinp; dz = g.cosp;
+            area = (float)g.area;
+            if (M.opaque) necl += disc_eclipse(M, M.rdisc1_g, px, py, pz, ing + necl, eg + necl);
+            if (M.eclipse1) star_ecl(1, px, py, pz);
+            if (M.eclipse2) star_ecl(2, px, py, pz);
+            double r = sqrt(px * px + py * py + pz * pz);
+            flux = (float)(M.disc_bright * pow(r / M.rdisc2, M.texp_disc) * (double)area);
+        } else if (sg.kind == SEG_EDGE) {  // grid.rs:411-478, brightness.rs:215-239
+            const int64_t col = i / M.edge_nout, row = i - col * M.edge_nout;
+            double th = kTwoPi * (double)col / (double)M.edge_ntheta;
+            double st, ct;
+            sincos(th, &st, &ct);
+            const double rv = M.edge_rad, h = M.edge_h;
+            if (row == 0) {
+                px = kEfac * rv * ct; py = kEfac * rv * st; pz = kEfac * h;
+                area = (float)(M.edge_area / 2.0);
+            } else {
+                pz = -h + 2.0 * h * (double)(row - 1) / (double)(M.edge_nout - 1);
+                px = kEfac * rv * ct; py = kEfac * rv * st;
+                area = (float)M.edge_area;
+            }
+            dx = ct; dy = st; dz = 0.0;
+            if (M.opaque) necl += disc_eclipse(M, M.rdisc1_g, px, py, pz, ing + necl, eg + necl);
+            if (M.eclipse1) star_ecl(1, px, py, pz);
+            if (M.eclipse2) star_ecl(2, px, py, pz);
+            double vx = 1.0 - px, vy = -py, vz = -pz;
+            double r = sqrt(vx * vx + vy * vy + vz * vz);
+            double mu = (dx * vx + dy * vy + dz * vz) / r;
+            double temp, r2 = M.r2e, t4 = sq(M.tedge) * sq(M.tedge), i4 = sq(M.t2abs) * sq(M.t2abs);
+            if (mu >= r2) {
+                double geom = sq(r2 / r) * mu;
+                temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
+            } else if (mu > -r2) {
+                double x0 = -mu / r2;
+                double geom = sq(r2 / r) * r2 * (sqrt(1.0 - x0 * x0) * (2.0 + x0 * x0) / 3.0 - x0 * (kPi / 2.0 - asin(x0))) / kPi;
+                temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
+            } else {
+                temp = M.tedge;
+            }
+            flux = (float)((double)area * planck_d(M.wavelength, temp));
+        } else {  // SEG_SPOT: grid.rs:520-550
+            const int64_t k = i >> 1;
+            const bool tilted = (i & 1) == 0;
+            double dist = M.sfac_spot * (double)k / (double)(M.nspot - 1);
+            double f = M.length_spot * (dist - M.bmax);
+            px = M.bspot[0] + f * M.bvec[0]; py = M.bspot[1] + f * M.bvec[1]; pz = M.bspot[2] + f * M.bvec[2];
+            if (M.eclipse1) star_ecl(1, px, py, pz);
+            if (M.eclipse2) star_ecl(2, px, py, pz);
+            double bright = M.bright_ref * pow(dist / M.bmax, M.expon_spot) *
+                            exp(M.expon_spot / M.epow_spot - pow(dist, M.epow_spot));
+            area = (float)M.area_spot;
+            if (tilted) { dx = M.tvec[0]; dy = M.tvec[1]; dz = M.tvec[2]; flux = (float)(bright * (1.0 - M.cfrac_spot) * M.area_spot); }
+            else { dx = 0.0; dy = 0.0; dz = 1.0; flux = (float)(bright * M.cfrac_spot * M.area_spot); }
+        }
+        // outputs
+        A.el_rec[sg.first + i] = make_float4((float)dx, (float)dy, (float)dz, flux);
+        A.el_pos[sg.first + i] = make_float4((float)px, (float)py, (float)pz, 0.f);
+        double2* e = A.el_ecl + (sg.first + i) * kMaxEcl;
+        for (int k = 0; k < kMaxEcl; ++k)
+            e[k] = k < necl ? make_double2(ing[k], eg[k]) : make_double2(INFINITY, -INFINITY);
+        if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
+    }
+
+    // ---- per-model FP64 reductions (star segments only; block-uniform branch)
+    if (sg.kind != SEG_STAR1 && sg.kind != SEG_STAR2) return;
+    const int star = sg.kind == SEG_STAR1 ? 1 : 2;
+    double vals[16];
+    int slot[16];
+    int nv = 0;
+    for (int s = 0; s < M.nspec; ++s) {
+        const SpecPhase& sp = M.spec[s];
+        if (sp.star != star) continue;
+        bool match = sg.role == ROLE_BOTH || (sg.role == ROLE_FINE) == (sp.fine != 0);
+        if (!match) continue;
+        double c = 0.0;
+        if (valid) {  // comp_star1 / comp_star2 at one phase (flux.rs:115-206)
+            bool vis = true;
+            int ne = sp.star_ecl_only ? nse : necl;
+            for (int k = 0; k < ne; ++k)
+                if ((sp.phi >= ing[k] && sp.phi <= eg[k]) || sp.phi <= eg[k] - 1.0) vis = false;
+            double mu = sp.ex * dx + sp.ey * dy + sp.ez * dz;
+            const double* ld = star == 1 ? M.ld1 : M.ld2;
+            int lt = star == 1 ? M.ltype1 : M.ltype2;
+            double beam = star == 1 ? M.beam1 : M.beam2;
+            if (vis && mu > (star == 1 ? M.mucrit1 : M.mucrit2)) {
+                double mag = (star == 2 && M.glens1) ? lens_mag_d(px, py, pz, sp.ex, sp.ey, sp.ez, M.rlens1) : 1.0;
+                if (beam != 0.0) {
+                    double vxx = -M.vfac * py, vyy = M.vfac * (px - M.xcofm);
+                    double vr = -(sp.ex * vxx + sp.ey * vyy), vn = dx * vxx + dy * vyy;
+                    double mud = mu - mu * vr - vn;
+                    c = mu * mag * (double)flux * (1.0 - beam * vr) * imu_d(ld, lt, mud);
+                } else {
+                    c = mu * mag * (double)flux * imu_d(ld, lt, mu);
+                }
+            }
+        }
+        vals[nv] = c;
+        slot[nv] = AUX_SPEC0 + s;
+        ++nv;
+    }
+    if (sg.fine_star) {
+        double fg = valid ? (double)flux * (double)grav : 0.0, ff = valid ? (double)flux : 0.0;
+        double sa = 0.0, vol = 0.0;
+        if (valid) {
+            double cx = star == 1 ? 0.0 : 1.0;
+            double wx = px - cx, wy = py, wz = pz;
+            double r = sqrt(wx * wx + wy * wy + wz * wz);
+            double rc = dx * wx + dy * wy + dz * wz;
+            sa = (double)area * rc / ((r * r) * r);
+            vol = (double)area * rc;
+        }
+        vals[nv] = fg; slot[nv++] = star == 1 ? AUX_FG1 : AUX_FG2;
+        vals[nv] = ff; slot[nv++] = star == 1 ? AUX_F1 : AUX_F2;
+        vals[nv] = sa; slot[nv++] = star == 1 ? AUX_SA1 : AUX_SA2;
+        vals[nv] = vol; slot[nv++] = star == 1 ? AUX_VOL1 : AUX_VOL2;
+    }
+    if (nv == 0) return;
+    __shared__ double red[16][kElemThreads / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < nv; ++k) {
+        double v = vals[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double s = 0.0;
+        for (int w = 0; w < kElemThreads / 32; ++w) s += red[threadIdx.x][w];
+        atomicAdd(A.aux + (int64_t)sg.model * kNumAux + slot[threadIdx.x], s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_phase
+// ---------------------------------------------------------------------------
+__global__ void k_phase(PhaseArgs A) {
+    for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < A.ndatum;
+         d += (int64_t)gridDim.x * blockDim.x) {
+        const ModelDev& M = A.models[A.dmodel[d]];
+        if (M.status < 0) continue;
+        const lcb_datum D = A.data[d];
+        double phase = (D.time - M.t0) / M.period;
+        for (int k = 0; k < 4; ++k)
+            phase -= (M.t0 + phase * (M.period + M.pdot * phase) - D.time) / (M.period + 2.0 * M.pdot * phase);
+        phase += M.deltat / M.period / 2.0 * (cos(2.0 * kPi * phase) - 1.0);
+        double expose = D.expose / M.period;
+        double frac = (D.time - M.middle) / M.range;
+        A.d_slfac[d] = 1.0 + frac * (M.slope + frac * (M.quad + frac * M.cube));
+        int64_t j = A.dsub0[d];
+        for (int nd = 0; nd < D.ndiv; ++nd, ++j) {
+            double phi = phase, w = 1.0;
+            if (D.ndiv != 1) {
+                phi = phase + expose * ((double)nd - (double)(D.ndiv - 1) / 2.0) / (double)(D.ndiv - 1);
+                w = (nd == 0 || nd == D.ndiv - 1) ? 0.5 : 1.0;
+            }
+            double sn, cs;
+            sincos(kTwoPi * phi, &sn, &cs);
+            A.sp_e[j] = make_float4((float)(M.sini_l * cs), (float)(-M.sini_l * sn), (float)M.cosi_l, 0.f);
+            double pn = phi - floor(phi);
+            A.sp_phi[j] = pn;
+            int t = (pn <= M.phase1 || pn >= 1.0 - M.phase1) ? 1
+                    : (((pn > M.phase1 && pn < M.phase2) || (pn > 1.0 - M.phase2 && pn < 1.0 - M.phase1)) ? 2 : 3);
+            A.sp_type[j] = (int8_t)t;
+            A.sp_w[j] = w;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_flux
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}" : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait (about 2 s of SM clock); on time-out the caller records an error.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    long long t0 = clock64();
+    while (!mbar_test(bar, parity)) {
+        __nanosleep(64);
+        if (clock64() - t0 > 4000000000LL) return false;
+    }
+    return true;
+}
+
+enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
+
+struct FluxSmem {
+    float4 rec[2][kFluxChunk];
+    float4 pos[2][kFluxChunk];
+    double2 ecl[2][kFluxChunk * kMaxEcl];
+    int8_t cls[kFluxChunk];
+    uint64_t bar[2];
+    int unit;
+};
+
+size_t flux_smem_bytes_impl() { return sizeof(FluxSmem); }
+
+// Range classification of one eclipse pair against [lo, hi] (exact in FP64).
+__device__ __forceinline__ int pair_cls(double ing, double eg, double lo, double hi) {
+    if ((ing <= lo && hi <= eg) || hi <= eg - 1.0) return CLS_HID;
+    if ((hi < ing || lo > eg) && lo > eg - 1.0) return CLS_VIS;
+    return CLS_MIX;
+}
+
+__device__ __forceinline__ int classify(const double2* e, const double* rlo, const double* rhi) {
+    int res = -1;
+    for (int h = 0; h < 2; ++h) {
+        if (!(rlo[h] <= rhi[h])) continue;  // empty half
+        int c = CLS_VIS;
+        for (int k = 0; k < kMaxEcl; ++k) {
+            double2 p = e[k];
+            if (!(p.x <= 2.0)) break;  // unused pair
+            int pc = pair_cls(p.x, p.y, rlo[h], rhi[h]);
+            if (pc == CLS_HID) { c = CLS_HID; break; }
+            if (pc == CLS_MIX) c = CLS_MIX;
+        }
+        if (res < 0) res = c;
+        else if (res != c) res = CLS_MIX;
+    }
+    return res < 0 ? CLS_HID : res;
+}
+
+__device__ __forceinline__ bool hidden_at(const double2* e, double phi) {
+    bool h = false;
+    for (int k = 0; k < kMaxEcl; ++k) {
+        double2 p = e[k];
+        if (!(p.x <= 2.0)) break;
+        h |= (phi >= p.x && phi <= p.y) || phi <= p.y - 1.0;
+    }
+    return h;
+}
+
+// Per-kind contribution of one element at one sub-phase (FP32).
+template <int KIND>
+struct Contrib {
+    float a0, a1, a2, a3, thr, sumc;  // LD coefficients, mu threshold, sum of Claret coefficients
+    __device__ void setup(const ModelDev& M, int star) {
+        const float* l = star == 1 ? M.ld1f : M.ld2f;
+        a0 = l[0]; a1 = l[1]; a2 = l[2]; a3 = l[3];
+        float mc = star == 1 ? M.mucrit1f : M.mucrit2f;
+        thr = fmaxf(mc, 0.f);
+        sumc = a0 + a1 + a2 + a3;
+        if (KIND == UK_DISC) { a0 = M.lin_ldf; a1 = M.quad_ldf; thr = 0.f; }
+        if (KIND == UK_SPOT) thr = 0.f;
+    }
+    __device__ __forceinline__ float operator()(float mu, float fl) const {
+        if (KIND == UK_SPOT) return mu * fl;
+        if (KIND == UK_DISC) {
+            float om = 1.f - mu;
+            return mu * fl * (1.f - om * (a0 + a1 * om));
+        }
+        if (KIND == UK_STAR_CLARET) {
+            float m = fminf(mu, 1.f);
+            float ms = m * rsqrtf(m);
+            float im = (1.f - sumc) + ms * (a0 + ms * (a1 + ms * (a2 + ms * a3)));
+            return mu * fl * im;
+        }
+        float om = 1.f - fminf(mu, 1.f);
+        float p;
+        if (KIND == UK_STAR_POLY1) p = a0;
+        else if (KIND == UK_STAR_POLY2) p = a0 + om * a1;
+        else if (KIND == UK_STAR_POLY3) p = a0 + om * (a1 + om * a2);
+        else p = a0 + om * (a1 + om * (a2 + om * a3));
+        return mu * fl * (1.f - om * p);
+    }
+};
+
+// FP32 LDC::imu for the beaming path (types.rs:101-119)
+__device__ __forceinline__ float imu_f(const float* l, int lt, float mu) {
+    if (mu <= 0.f) return 0.f;
+    mu = fminf(mu, 1.f);
+    float om = 1.f - mu;
+    if (lt == 0) return 1.f - om * (l[0] + om * (l[1] + om * (l[2] + om * l[3])));
+    float ms = mu * rsqrtf(mu);
+    return (1.f - (l[0] + l[1] + l[2] + l[3])) + ms * (l[0] + ms * (l[1] + ms * (l[2] + ms * l[3])));
+}
+
+template <int KIND>
+__device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uint32_t* parity) {
+    const ModelDev& M = A.models[U.model];
+    const int tid = threadIdx.x;
+    const int64_t sbase = M.sub_begin + U.t0;
+    // ---- the tile's sub-phases in registers
+    float ex[kFluxR], ey[kFluxR], ez[kFluxR];
+    double ph[kFluxR];
+    bool act[kFluxR];
+    double dlo[2] = {2.0, 2.0}, dhi[2] = {-1.0, -1.0};
+#pragma unroll
+    for (int k = 0; k < kFluxR; ++k) {
+        int j = tid + k * kFluxThreads;
+        act[k] = false;
+        ex[k] = ey[k] = ez[k] = 0.f;
+        ph[k] = -1.0;
+        if (j < U.nt) {
+            int t = A.sp_type[sbase + j];
+            bool a = true;
+            if (U.star == 1) a = U.role == ROLE_BOTH || ((U.role == ROLE_FINE) == (t == 1));
+            else if (U.star == 2) a = U.role == ROLE_BOTH || ((U.role == ROLE_FINE) == (t == 3));
+            if (a) {
+                float4 e = A.sp_e[sbase + j];
+                ex[k] = e.x; ey[k] = e.y; ez[k] = e.z;
+                ph[k] = A.sp_phi[sbase + j];
+                act[k] = true;
+                int h = ph[k] >= 0.5 ? 1 : 0;
+                dlo[h] = fmin(dlo[h], ph[k]);
+                dhi[h] = fmax(dhi[h], ph[k]);
+            }
+        }
+    }
+    // block min/max of the two halves
+    for (int h = 0; h < 2; ++h) {
+        double a = dlo[h], b = dhi[h];
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+        }
+        dlo[h] = a; dhi[h] = b;
+    }
+    __shared__ double s_lo[kFluxThreads / 32][2], s_hi[kFluxThreads / 32][2];
+    if ((tid & 31) == 0) {
+        s_lo[tid >> 5][0] = dlo[0]; s_lo[tid >> 5][1] = dlo[1];
+        s_hi[tid >> 5][0] = dhi[0]; s_hi[tid >> 5][1] = dhi[1];
+    }
+    __syncthreads();
+    double rlo[2] = {2.0, 2.0}, rhi[2] = {-1.0, -1.0};
+    for (int w = 0; w < kFluxThreads / 32; ++w)
+        for (int h = 0; h < 2; ++h) { rlo[h] = fmin(rlo[h], s_lo[w][h]); rhi[h] = fmax(rhi[h], s_hi[w][h]); }
+    const bool any = rlo[0] <= rhi[0] || rlo[1] <= rhi[1];
+
+    float acc_hi[kFluxR], acc_lo[kFluxR];
+#pragma unroll
+    for (int k = 0; k < kFluxR; ++k) acc_hi[k] = acc_lo[k] = 0.f;
+
+    Contrib<KIND> C;
+    C.setup(M, U.star);
+    const bool need_pos = KIND == UK_STAR_GENERIC;
+    // generic-path constants
+    const float* ldg = U.star == 1 ? M.ld1f : M.ld2f;
+    const int ltg = U.star == 1 ? M.ltype1 : M.ltype2;
+    const float beam = U.star == 1 ? M.beam1f : M.beam2f;
+    const float spin = U.star == 1 ? M.spin1f : M.spin2f;
+    const float thrg = U.star == 1 ? M.mucrit1f : M.mucrit2f;  // see(mu) without the mu > 0 shortcut
+    const bool lens = U.star == 2 && M.glens1;
+
+    const int nchunks = any ? (U.ne + kFluxChunk - 1) / kFluxChunk : 0;
+    auto issue = [&](int c) {
+        int b = c & 1;
+        int64_t e0 = U.e0 + (int64_t)c * kFluxChunk;
+        int n = min(kFluxChunk, U.ne - c * kFluxChunk);
+        uint32_t bytes = (uint32_t)n * (16u + 16u * kMaxEcl + (need_pos ? 16u : 0u));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect(&S.bar[b], bytes);
+        bulk_load(S.rec[b], A.el_rec + e0, (uint32_t)n * 16u, &S.bar[b]);
+        bulk_load(S.ecl[b], A.el_ecl + e0 * kMaxEcl, (uint32_t)n * 16u * kMaxEcl, &S.bar[b]);
+        if (need_pos) bulk_load(S.pos[b], A.el_pos + e0, (uint32_t)n * 16u, &S.bar[b]);
+    };
+    if (tid == 0) {
+        if (nchunks > 0) issue(0);
+        if (nchunks > 1) issue(1);
+    }
+    for (int c = 0; c < nchunks; ++c) {
+        const int b = c & 1;
+        const int n = min(kFluxChunk, U.ne - c * kFluxChunk);
+        if (!mbar_wait(&S.bar[b], parity[b])) atomicOr(A.status + U.model, kStatusTmaTimeout);
+        parity[b] ^= 1u;
+        for (int e = tid; e < n; e += kFluxThreads) S.cls[e] = (int8_t)classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
+        __syncthreads();
+        for (int s0 = 0; s0 < n; s0 += 32) {
+            float part[kFluxR];
+#pragma unroll
+            for (int k = 0; k < kFluxR; ++k) part[k] = 0.f;
+            const int s1 = min(s0 + 32, n);
+            for (int e = s0; e < s1; ++e) {
+                const int cls = S.cls[e];
+                if (cls == CLS_HID) continue;
+                const float4 r = S.rec[b][e];
+                if (KIND == UK_STAR_GENERIC) {
+                    const float4 p = S.pos[b][e];
+                    float vx, vy;
+                    if (U.star == 1) { vx = -M.vfacf * spin * p.y; vy = M.vfacf * (spin * p.x - M.xcofmf); }
+                    else { vx = -M.vfacf * spin * p.y; vy = M.vfacf * (spin * (p.x - 1.f) + 1.f - M.xcofmf); }
+                    const float vn = r.x * vx + r.y * vy;
+#pragma unroll
+                    for (int k = 0; k < kFluxR; ++k) {
+                        float mu = ex[k] * r.x + ey[k] * r.y + ez[k] * r.z;
+                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(&S.ecl[b][e * kMaxEcl], ph[k]));
+                        if (v) {
+                            float mag = 1.f;
+                            if (lens) {
+                                float d = -(p.x * ex[k] + p.y * ey[k] + p.z * ez[k]);
+                                if (d > 0.f) {
+                                    float ax = p.x + d * ex[k], ay = p.y + d * ey[k], az = p.z + d * ez[k];
+                                    float pp = sqrtf(ax * ax + ay * ay + az * az), phh = pp * 0.5f, phsq = phh * phh;
+                                    float rd = M.rlens1f * d;
+                                    float pd = phsq > 25.f * rd ? pp + rd / pp : phh + sqrtf(phsq + rd);
+                                    mag = pd * pd / (pd - phh) / phh * 0.25f;
+                                }
+                            }
+                            if (beam != 0.f) {
+                                float vr = -(ex[k] * vx + ey[k] * vy);
+                                float mud = mu - mu * vr - vn;
+                                part[k] += mu * mag * r.w * (1.f - beam * vr) * imu_f(ldg, ltg, mud);
+                            } else {
+                                part[k] += mu * mag * r.w * imu_f(ldg, ltg, mu);
+                            }
+                        }
+                    }
+                } else if (cls == CLS_VIS) {
+#pragma unroll
+                    for (int k = 0; k < kFluxR; ++k) {
+                        float mu = fmaf(ez[k], r.z, fmaf(ey[k], r.y, ex[k] * r.x));
+                        if (mu > C.thr) part[k] += C(mu, r.w);
+                    }
+                } else {
+                    const double2* ee = &S.ecl[b][e * kMaxEcl];
+#pragma unroll
+                    for (int k = 0; k < kFluxR; ++k) {
+                        float mu = fmaf(ez[k], r.z, fmaf(ey[k], r.y, ex[k] * r.x));
+                        if (mu > C.thr && !hidden_at(ee, ph[k])) part[k] += C(mu, r.w);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kFluxR; ++k) {  // two-sum fold of the 32-element block
+                float s = acc_hi[k] + part[k];
+                float bb = s - acc_hi[k];
+                float err = (acc_hi[k] - (s - bb)) + (part[k] - bb);
+                acc_hi[k] = s;
+                acc_lo[k] += err;
+            }
+        }
+        __syncthreads();  // everyone is done with buffer b
+        if (tid == 0 && c + 2 < nchunks) issue(c + 2);
+    }
+    // ---- write the partial sums of this (slot, tile)
+    double* out = A.partial + M.pbase + (int64_t)U.slot * M.nsub + U.t0;
+#pragma unroll
+    for (int k = 0; k < kFluxR; ++k) {
+        int j = tid + k * kFluxThreads;
+        if (j < U.nt) out[j] = act[k] ? (double)acc_hi[k] + (double)acc_lo[k] : 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(kFluxThreads, 4) k_flux(FluxArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    FluxSmem& S = *reinterpret_cast<FluxSmem*>(smem_raw);
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0]);
+        mbar_init(&S.bar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity[2] = {0u, 0u};
+    for (;;) {
+        if (threadIdx.x == 0) S.unit = atomicAdd(A.counter, 1);
+        __syncthreads();
+        const int64_t u = S.unit;
+        __syncthreads();
+        if (u >= A.nunits) break;
+        const FluxUnit U = A.units[u];
+        switch (U.kind) {
+            case UK_STAR_POLY1: flux_unit<UK_STAR_POLY1>(A, U, S, parity); break;
+            case UK_STAR_POLY2: flux_unit<UK_STAR_POLY2>(A, U, S, parity); break;
+            case UK_STAR_POLY3: flux_unit<UK_STAR_POLY3>(A, U, S, parity); break;
+            case UK_STAR_POLY4: flux_unit<UK_STAR_POLY4>(A, U, S, parity); break;
+            case UK_STAR_CLARET: flux_unit<UK_STAR_CLARET>(A, U, S, parity); break;
+            case UK_STAR_GENERIC: flux_unit<UK_STAR_GENERIC>(A, U, S, parity); break;
+            case UK_DISC: flux_unit<UK_DISC>(A, U, S, parity); break;
+            default: flux_unit<UK_SPOT>(A, U, S, parity); break;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_epilogue
+// ---------------------------------------------------------------------------
+struct Gint {  // types.rs:130-202
+    double p1, p2, s11, s12, s21, s22;
+    __device__ double scale1(double phase) const {
+        double pn = phase - floor(phase);
+        if (pn <= p1 || pn >= 1.0 - p1) return 1.0;
+        return (s11 * (1.0 - p1 - pn) + s12 * (pn - p1)) / (1.0 - 2.0 * p1);
+    }
+    __device__ double scale2(double phase) const {
+        double pn = phase - floor(phase);
+        if (pn >= p2 && pn <= 1.0 - p2) return 1.0;
+        if (pn < 0.5) return (s22 * (p2 - pn) + s21 * (pn + p2)) / (2.0 * p2);
+        return (s21 * (1.0 + p2 - pn) + s22 * (pn - 1.0 + p2)) / (2.0 * p2);
+    }
+};
+
+constexpr int kEpiThreads = 256;
+
+__device__ double block_sum(double v, double* red) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int w = 0; w < kEpiThreads / 32; ++w) s += red[w];
+    return s;
+}
+
+__global__ void __launch_bounds__(kEpiThreads) k_epilogue(EpiArgs A) {
+    const int64_t m = blockIdx.x;
+    const ModelDev& M = A.models[m];
+    double* res = A.results + m * 12;
+    __shared__ double red[kEpiThreads / 32];
+    __shared__ Gint G;
+    __shared__ double s_wd;
+    if (M.status < 0 || A.status[m] != 0) {
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 12; ++k) res[k] = NAN;
+        }
+        for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) A.calc[M.datum_begin + d] = NAN;
+        return;
+    }
+    const double* aux = A.aux + m * kNumAux;
+    if (threadIdx.x == 0) {  // orchestration.rs:86-131 with the live Ginterp
+        Gint g{M.phase1, M.phase2, 1.0, 1.0, 1.0, 1.0};
+        auto c1 = [&](int s) { return g.scale1(M.spec[s].phase) * aux[AUX_SPEC0 + s]; };
+        auto c2 = [&](int s) { return g.scale2(M.spec[s].phase) * aux[AUX_SPEC0 + s]; };
+        if (!M.copy1) {
+            g.s11 = c1(M.spec_g11[0]) / c1(M.spec_g11[1]);
+            g.s12 = c1(M.spec_g12[0]) / c1(M.spec_g12[1]);
+        }
+        if (!M.copy2) {
+            g.s21 = c2(M.spec_g21[0]) / c2(M.spec_g21[1]);
+            g.s22 = c2(M.spec_g22[0]) / c2(M.spec_g22[1]);
+        }
+        G = g;
+        s_wd = g.scale1(0.5) * aux[AUX_SPEC0 + M.spec_wd];
+    }
+    __syncthreads();
+    const Gint g = G;
+    const double* P = A.partial + M.pbase;
+    double chi = 0.0, wnok = 0.0, sdy = 0.0, syy = 0.0;
+    for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+        const int64_t gd = M.datum_begin + d;
+        const lcb_datum D = A.data[gd];
+        int64_t j = A.dsub0[gd] - M.sub_begin;
+        double sum = 0.0;
+        for (int nd = 0; nd < D.ndiv; ++nd, ++j) {
+            double pn = A.sp_phi[M.sub_begin + j];
+            double s1 = 0.0, s2 = 0.0, s0 = 0.0;
+            for (int s = 0; s < M.g1_end; ++s) s1 += P[(int64_t)s * M.nsub + j];
+            for (int s = M.g1_end; s < M.g2_end; ++s) s2 += P[(int64_t)s * M.nsub + j];
+            for (int s = M.g2_end; s < M.nslots; ++s) s0 += P[(int64_t)s * M.nsub + j];
+            double ss = s1 * g.scale1(pn);
+            ss += g.scale2(pn) * s2;
+            ss += s0;
+            sum += A.sp_w[M.sub_begin + j] * ss;
+        }
+        double c = A.d_slfac[gd] * (sum / (double)max(1, D.ndiv - 1)) + M.third;
+        A.calc[gd] = c;
+        if (D.weight > 0.0) {
+            if (A.scale) {
+                double w = D.weight / sq(D.ferr);
+                sdy += w * D.flux * c;
+                syy += w * c * c;
+                wnok += D.weight;
+            } else if (A.rdata) {
+                wnok += D.weight;
+                chi += D.weight * sq((D.flux - c) / D.ferr);
+            }
+        }
+    }
+    double sfac = 1.0;
+    if (A.scale) {  // re_scale (orchestration.rs:361-388)
+        sdy = block_sum(sdy, red);
+        syy = block_sum(syy, red);
+        wnok = block_sum(wnok, red);
+        if (wnok > 0.0 && syy > 0.0) {
+            sfac = sdy / syy;
+            chi = 0.0;
+            for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+                const int64_t gd = M.datum_begin + d;
+                const lcb_datum D = A.data[gd];
+                double c = A.calc[gd] * sfac;
+                A.calc[gd] = c;
+                if (D.weight > 0.0) chi += D.weight * sq((D.flux - c) / D.ferr);
+            }
+            chi = block_sum(chi, red);
+        } else {
+            chi = 0.0;
+            wnok = 0.0;
+        }
+    } else {
+        chi = block_sum(chi, red);
+        wnok = block_sum(wnok, red);
+    }
+    if (threadIdx.x == 0) {
+        res[0] = s_wd * sfac;
+        res[1] = chi;
+        res[2] = wnok;
+        double fg1 = aux[AUX_FG1], f1 = aux[AUX_F1], fg2 = aux[AUX_FG2], f2 = aux[AUX_F2];
+        res[3] = (M.glogg1 > 0.0 && fg1 > 0.0 && f1 > 0.0) ? log10(M.glogg1 * fg1 / f1) : 0.0;
+        res[4] = (M.glogg2 > 0.0 && fg2 > 0.0 && f2 > 0.0) ? log10(M.glogg2 * fg2 / f2) : 0.0;
+        res[5] = pow(aux[AUX_VOL1] / aux[AUX_SA1], 1.0 / 3.0);
+        res[6] = pow(aux[AUX_VOL2] / aux[AUX_SA2], 1.0 / 3.0);
+        for (int k = 0; k < 5; ++k) res[7 + k] = sfac;
+    }
+}
+
+}  // namespace
+
+size_t flux_smem_bytes() { return flux_smem_bytes_impl(); }
+
+// The flux kernel's dynamic shared memory exceeds the 48 KB default; the
+// attribute is set once per process (outside any stream capture).
+cudaError_t configure_flux() {
+    static cudaError_t status = cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)flux_smem_bytes());
+    return status;
+}
+
+int flux_blocks_per_sm() {
+    if (configure_flux() != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_flux, kFluxThreads, flux_smem_bytes()) != cudaSuccess) return 0;
+    return n;
+}
+
+cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s) {
+    if (a.ndatum <= 0) return cudaSuccess;
+    int64_t blocks = (a.ndatum + 255) / 256;
+    if (blocks > 65535 * 8) blocks = 65535 * 8;
+    k_phase<<<(unsigned)blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_elements(const ElemArgs& a, cudaStream_t s) {
+    if (a.nblocks <= 0) return cudaSuccess;
+    k_elements<<<(unsigned)a.nblocks, kElemThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flux(const FluxArgs& a, int grid, cudaStream_t s) {
+    if (a.nunits <= 0) return cudaSuccess;
+    cudaError_t e = configure_flux();
+    if (e != cudaSuccess) return e;
+    k_flux<<<grid, kFluxThreads, flux_smem_bytes(), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_epilogue(const EpiArgs& a, cudaStream_t s) {
+    if (a.nmodels <= 0) return cudaSuccess;
+    k_epilogue<<<(unsigned)a.nmodels, kEpiThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace lcb

@@ -1,0 +1,43 @@
+// lcb_plan.h — host planning of a batch: per-model constants and work decomposition.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "lcb_internal.h"
+#include "lcb_model.h"
+
+namespace lcb {
+
+struct Plan {
+    std::vector<ModelDev> models;
+    std::vector<SegDesc> segs;
+    std::vector<Band> bands;
+    std::vector<Ring> rings;
+    std::vector<ElemBlock> eblocks;
+    std::vector<FluxUnit> units;
+    std::vector<int32_t> datum_model;   // per (model, datum): model index
+    std::vector<int64_t> datum_sub0;    // per (model, datum): first global sub-phase
+    std::vector<int64_t> datum_src;     // per (model, datum): index into the caller's data array
+    std::vector<int32_t> model_ok;      // 1 = planned, 0 = failed (NaN chisq)
+    std::vector<std::string> model_err;
+    int64_t nelem = 0, nsub = 0, ndatum = 0, npartial = 0;
+    int64_t evals = 0, roche_elems = 0;
+    // Signature of everything that fixes buffer sizes and launch shapes.
+    std::vector<int64_t> shape_key;
+};
+
+// Plans models[0..n); model i is evaluated on data[start[i] .. start[i]+count[i])
+// (ranges may overlap, e.g. one shared data set).  Models that are physically
+// invalid are marked failed (model_ok = 0) instead of throwing.
+void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, const int64_t* start,
+                const int64_t* count, int num_sms, Plan& out);
+
+// Host FP64 helpers also used by tests of the planner.
+double host_xl1(double q);
+double host_xl11(double q, double spin);
+double host_xl12(double q, double spin);
+void host_stream_spot(double q, double radius, double out[3]);
+int64_t host_numface(int nlat);
+
+}  // namespace lcb

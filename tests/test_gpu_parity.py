@@ -1,0 +1,154 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle and the
+reference's golden vectors.  Tolerance: max relative error 1e-5 on fluxes
+(the FP32 flux sum with compensated accumulation against the FP64 oracle).
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def W():
+    return importlib.import_module("lcurve-rs_b200.workloads")
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
+
+
+def gpu_and_oracle_lc(lcb, oracle, text, times, expose, ndiv, scale=False, rdata=False, data=None):
+    d = data if data is not None else lcb.make_data(times, expose=expose, ndiv=ndiv, ferr=1.0, weight=1.0)
+    m = lcb.Model(text=text)
+    calc = np.zeros(d.shape[0])
+    import ctypes as C
+    res = lcb.Result()
+    lcb._capi.check(lcb._capi.load().lcb_light_curve(lcb._ctx(), m._h, d.ctypes.data, d.shape[0], int(scale),
+                                                     int(rdata), lcb._capi.dptr(calc), C.byref(res)))
+    o = oracle.Model(text=text).light_curve(d, scale=scale, rdata=rdata, nthreads=8)
+    return calc, res, o
+
+
+def test_golden_cpp_light_curve(lcb):
+    m = lcb.Model(GOLDEN / "test_model.dat")
+    r = m.light_curve(time1=-0.2, time2=1.2, ntime=500, expose=0.001, ndiv=1)
+    g = np.loadtxt(GOLDEN / "test_lc.dat")
+    assert rel_err(r.flux, g[:, 2]) < TOL
+    assert np.array_equal(r.times, g[:, 0])
+
+
+def test_golden_model_matches_oracle_scalars(lcb, oracle):
+    text = (GOLDEN / "test_model.dat").read_text()
+    t = np.linspace(-0.2, 1.2, 500)
+    calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, 0.001, 1)
+    assert rel_err(calc, o["calc"]) < TOL
+    assert abs(res.wdwarf - o["wdwarf"]) <= 1e-9 * abs(o["wdwarf"])
+    assert abs(res.rv1 - o["rv1"]) < 1e-12 and abs(res.rv2 - o["rv2"]) < 1e-12
+    assert res.logg1 == o["logg1"] and res.logg2 == o["logg2"]
+
+
+def test_single_small_vs_oracle(lcb, oracle, W):
+    text, t, expose, ndiv = W.single_small()
+    calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, expose, ndiv)
+    assert rel_err(calc, o["calc"]) < TOL
+
+
+def test_disc_edge_spot_irradiation_vs_oracle(lcb, oracle, W):
+    text, t, expose, ndiv = W.single_large(nlat1=40, nlat2=80, ntime=1500, nrad=50, nspot=40)
+    calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, expose, ndiv)
+    assert rel_err(calc, o["calc"]) < TOL
+    assert abs(res.wdwarf - o["wdwarf"]) <= 1e-7 * abs(o["wdwarf"])
+
+
+def test_lensing_spots_vs_oracle(lcb, oracle, W):
+    text, t, expose, ndiv = W.single_huge(nlat1=40, nlat2=80, ntime=800, nrad=50)
+    calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, expose, ndiv)
+    assert rel_err(calc, o["calc"]) < TOL
+
+
+def test_beaming_and_coarse_grids_vs_oracle(lcb, oracle, W):
+    text = W.model_text(velocity_scale=300.0, beam_factor1=1.3, beam_factor2=0.8, spin1=1.1, spin2=0.9,
+                        nlat1f=40, nlat1c=20, nlat2f=60, nlat2c=30, limb1="Claret", ldc1_1=0.5, ldc1_2=-0.2,
+                        ldc1_3=0.3, ldc1_4=-0.1, mucrit1=0.01)
+    t = np.linspace(-0.3, 1.3, 700)
+    calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, 0.003, 3)
+    assert rel_err(calc, o["calc"]) < TOL
+    assert abs(res.wdwarf - o["wdwarf"]) <= 1e-7 * abs(o["wdwarf"])
+
+
+def test_light_curve_scale_and_chisq(lcb, oracle, W):
+    text, t, expose, ndiv = W.single_small()
+    base = lcb.Model(text=text).light_curve(times=t, expose=expose, ndiv=ndiv).flux
+    d = W.noisy_data(t, 2.5 * base, expose, ndiv, seed=3)
+    for scale in (False, True):
+        calc, res, o = gpu_and_oracle_lc(lcb, oracle, text, t, expose, ndiv, scale=scale, rdata=True, data=d)
+        assert rel_err(calc, o["calc"]) < TOL
+        assert abs(res.chisq - o["chisq"]) <= 1e-4 * abs(o["chisq"])
+        assert res.wnok == o["wnok"]
+        assert np.allclose(list(res.sfac), o["sfac"], rtol=1e-5)
+
+
+def test_chisq_batch_vs_oracle(lcb, oracle):
+    # tests/chisq_batch.rs and crates/lcurve-cuda/tests/gpu_correctness.rs shapes
+    text = (GOLDEN / "test_model.dat").read_text()
+    t = np.linspace(-0.2, 1.2, 200)
+    d = lcb.make_data(t, expose=0.001, ndiv=1, flux=1.0e-9, ferr=1.0e-11, weight=1.0)
+    n = 16
+    frac = np.arange(n) / (n - 1) - 0.5
+    vals = np.stack([0.5 + 0.02 * frac, 82.0 + 2.0 * frac], axis=1)
+    m = lcb.Model(text=text)
+    o = oracle.Model(text=text)
+    for scale in (False, True):
+        g = m.chisq_batch(d, ["q", "iangle"], vals, scale=scale)
+        c = o.chisq_batch(d, ["q", "iangle"], vals, scale=scale, nthreads=8)
+        assert np.all(np.isfinite(g))
+        assert rel_err(g, c) < 1e-4
+
+
+def test_chisq_batch_unphysical_is_nan(lcb):
+    m = lcb.Model(GOLDEN / "test_model.dat")
+    d = lcb.make_data(np.linspace(-0.2, 1.2, 50), flux=0.0, ferr=1.0, weight=1.0)
+    out = m.chisq_batch(d, ["r2", "bogus"], np.array([[0.99, 1.0], [-1.0, 2.0]]), scale=False)
+    assert np.isnan(out[0]) and np.isfinite(out[1])
+
+
+def test_ragged_batch_and_resident_batch_vs_oracle(lcb, oracle, W):
+    specs = W.batch_models(n=6, seed=5, nlat1=(20, 40), nlat2=(30, 60), ntime=(150, 300))
+    models = [lcb.Model(text=s) for s, _ in specs]
+    fid = lcb.Model(text=W.single_small()[0])
+    datas, offs = [], [0]
+    for i, (_, t) in enumerate(specs):
+        f = fid.light_curve(times=t, expose=0.001, ndiv=1).flux
+        datas.append(W.noisy_data(t, f, 0.001, 1, seed=100 + i))
+        offs.append(offs[-1] + len(t))
+    data = np.concatenate(datas)
+    chi, calc, res = lcb.chisq_batch_ragged(models, data, offs, scale=False, want_calc=True)
+    ochi = oracle.chisq_ragged([oracle.Model(text=s) for s, _ in specs], data, offs, scale=False, nthreads=8)
+    assert rel_err(chi, ochi) < 1e-4
+    for i, (s, t) in enumerate(specs):
+        o = oracle.Model(text=s).light_curve(data[offs[i]:offs[i + 1]], rdata=True, nthreads=8)
+        assert rel_err(calc[offs[i]:offs[i + 1]], o["calc"]) < TOL
+    B = lcb.Batch(models, data, offs)
+    B.run(scale=False)
+    bchi, bcalc, _ = B.results(want_calc=True)
+    assert np.allclose(bchi, chi, rtol=1e-12, atol=0)
+    B.run(scale=False)  # graph replay
+    bchi2, _, _ = B.results()
+    assert np.allclose(bchi2, chi, rtol=1e-12, atol=0)
+    # parameter update without re-upload of data
+    q = np.array([m.q for m in models]) * 0.9
+    B.set_params(["q"], q[:, None])
+    B.run(scale=False)
+    bchi3, _, _ = B.results()
+    for i, (s, _) in enumerate(specs):
+        om = oracle.Model(text=s)
+        om.set("q", q[i])
+        c = om.light_curve(data[offs[i]:offs[i + 1]], rdata=True, nthreads=8)["chisq"]
+        assert abs(bchi3[i] - c) <= 1e-4 * abs(c)
