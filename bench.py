@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark: model evals/s of the 1024-model uneven chi-squared batch.
+
+One step = one evaluation of a batch of 1024 models (per GPU) with uneven grid
+sizes (nlat1f U{30..300}, nlat2f U{30..500}) and time counts (ntime
+U{200..5000}): grids, FP64 Roche eclipses, continuum, FP32 flux sum over all
+elements x times, chi-squared.  Inputs are seeded synthetic models and noisy
+data (lcurve-rs_b200/workloads.py).
+
+  value : device-resident throughput -- data uploaded once, each step replays
+          the captured launch sequence (lcb_batch_run); CUDA events on the
+          library's stream, max over ranks.
+  e2e   : the same batch through lcb_chisq_batch_ragged with the inputs in
+          pinned host memory: host planning, H2D of tables and data, kernels,
+          D2H of the results, every step.
+
+Multi-GPU (torchrun): weak scaling, each rank evaluates its own 1024-model
+batch (seed 1234 + rank); no collective on the data path, only the timing
+reduction.  `--impl reference` times the CPU oracle (the FP64 restatement of
+the reference's Rayon path) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "model evals/s (1024-model batch)"
+UNIT = "model evals/s"
+FLUX_FLOPS_PER_EVAL = 17     # dot 5 + limb darkening 9 + product 2 + accumulate 1
+POT_FLOPS_PER_EVAL = 22      # one Roche potential (or gradient) evaluation
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--models", type=int, default=1024)
+    p.add_argument("--cpu-sample", type=int, default=0, help="models per CPU-baseline step (0 = host threads)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-i",
+                 str(self.device), "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(lcb, W, n, seed):
+    specs = W.batch_models(n=n, seed=seed)
+    models = [lcb.Model(text=s) for s, _ in specs]
+    offs = np.zeros(n + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(t) for _, t in specs])
+    times = np.concatenate([t for _, t in specs])
+    # data = the single_small model's curve at each model's times + 1% noise
+    fid_text = W.single_small()[0]
+    fid = [lcb.Model(text=fid_text) for _ in range(n)]
+    tmpl = lcb.make_data(times, expose=0.001, ndiv=1, flux=1.0, ferr=1.0, weight=1.0)
+    _, fflux, _ = lcb.chisq_batch_ragged(fid, tmpl, offs, scale=False, want_calc=True)
+    rng = np.random.default_rng(seed + 99)
+    sig = 0.01 * np.abs(fflux)
+    data = lcb.make_data(times, expose=0.001, ndiv=1, flux=fflux + sig * rng.standard_normal(fflux.shape),
+                         ferr=sig, weight=1.0)
+    return specs, models, data, offs
+
+
+def cpu_models_per_s(specs, data, offs, first, count, nthreads):
+    from oracle import oracle as O
+    sel = [(first + k) % len(specs) for k in range(count)]
+    oms = [O.Model(text=specs[i][0]) for i in sel]
+    parts, o2 = [], [0]
+    for i in sel:
+        parts.append(data[offs[i]:offs[i + 1]])
+        o2.append(o2[-1] + offs[i + 1] - offs[i])
+    d = np.concatenate(parts)
+    t0 = time.perf_counter()
+    O.chisq_ragged(oms, d, o2, scale=False, nthreads=nthreads)
+    return count / (time.perf_counter() - t0)
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text()).get(kernel, {}).get("dram_bytes_per_launch_full_workload")
+    except (ValueError, OSError):
+        return None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    from oracle import oracle as O  # noqa: F401  (builds/loads the oracle)
+    nthreads = os.cpu_count() or 1
+    sample = args.cpu_sample or nthreads
+    specs = W.batch_models(n=args.models, seed=1234)
+    offs = np.zeros(len(specs) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(t) for _, t in specs])
+    times = np.concatenate([t for _, t in specs])
+    # chi-squared needs data; its values do not change the work
+    data = O.make_data(times, expose=0.001, ndiv=1, flux=1.0, ferr=0.01, weight=1.0)
+    rates = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_models_per_s(specs, data, offs, s * sample, sample, nthreads)
+        if s >= args.warmup:
+            rates.append(r)
+    v = float(np.mean(rates))
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"batch_{args.models}: uneven models (nlat1f U{{30..300}}, nlat2f U{{30..500}}, "
+                               f"ntime U{{200..5000}}), seed 1234", "sample_models_per_step": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"{sample} models per step of the 1024-model batch, all host threads "
+                                   "(oracle/lcurve_oracle.cpp, parallel over models as the reference's Rayon "
+                                   "chisq_batch)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
+    lcb = importlib.import_module("lcurve-rs_b200")
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    lcb.set_device(f"cuda:{local}")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    lcb.set_stream(stream.cuda_stream)  # the library's work and the timing events share this stream
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    specs, models, data, offs = build_workload(lcb, W, args.models, 1234 + rank)
+    B = lcb.Batch(models, data, offs)
+    st = B.stats()
+    for _ in range(args.warmup):
+        B.run(scale=False)
+
+    # ---- device-resident value
+    barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            B.run(scale=False)  # CUDA-graph replay
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1) / args.steps
+        # per-kernel device times: the same launch sequence issued directly with CUDA events
+        # between the kernels on this stream (events inside a graph carry no timing)
+        stage_names = ["phase", "elements", "roche", "aux", "flux", "epilogue"]
+        stage_acc = np.zeros(len(stage_names))
+        for _ in range(args.steps):
+            s = B.profile(scale=False)
+            stage_acc += np.array([s[k] for k in stage_names])
+        counts = B.search_counts()
+        barrier()
+    st = B.stats()
+    chi, _, _ = B.results()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.models / (ms_max / 1e3)
+    stage = stage_acc / args.steps
+
+    # ---- end-to-end through the C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(data.nbytes, dtype=torch.uint8, pin_memory=True)
+        pdata = pinned.numpy().view(lcb.DATUM_DTYPE)
+        pdata[:] = data
+        lcb.chisq_batch_ragged(models, pdata, offs, scale=False)  # warm the transient buffers
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(args.steps):
+            c2, _, _ = lcb.chisq_batch_ragged(models, pdata, offs, scale=False)
+        e1.record(stream)
+        barrier()
+        wall = (time.perf_counter() - w0) / args.steps * 1e3
+        h2d, d2h = lcb.transfer_bytes()
+        t = torch.tensor([max(e0.elapsed_time(e1) / args.steps, wall)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+        same = bool(np.allclose(c2, chi, rtol=1e-9, equal_nan=True))
+        e2e = {"value": world * args.models / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "matches_resident": same}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel
+    p64 = lcb.fma_peak_tflops(True)
+    p32 = lcb.fma_peak_tflops(False)
+    # FP64 work of the Roche search as executed: potential and gradient evaluations plus
+    # lower-bound nodes (each costs about one potential evaluation)
+    roche_flops = (counts["pot_evals"] + counts["dpot_evals"] + counts["bound_nodes"]) * POT_FLOPS_PER_EVAL
+    flux_flops = st["element_evals"] * FLUX_FLOPS_PER_EVAL
+    kernels = {
+        "k_roche": {"ms": stage[2], "flops": roche_flops, "peak": p64, "pipe": "fp64"},
+        "k_flux": {"ms": stage[4], "flops": flux_flops, "peak": p32, "pipe": "fp32"},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    k = kernels[dom]
+    ach = k["flops"] / (k["ms"] / 1e3) / 1e12
+    roof = {"kernel": dom, "bound": k["pipe"], "achieved": ach, "peak": k["peak"], "unit": "TFLOP/s",
+            "frac": ach / k["peak"] if k["peak"] else None, "traffic": traffic_from_profiles(dom),
+            "peak_source": f"measured {k['pipe'].upper()} FMA peak of this GPU (k_fma_peak); "
+                           "MEASURED_PEAKS.json has HBM and bf16 only",
+            "other": {n: {"ms": v["ms"], "achieved_tflops": v["flops"] / (v["ms"] / 1e3) / 1e12 if v["ms"] else None,
+                          "peak_tflops": v["peak"]} for n, v in kernels.items()}}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        sample = args.cpu_sample or nthreads
+        rate = cpu_models_per_s(specs, data, offs, 0, sample, nthreads)
+        cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"first {sample} models of the batch, all host threads, parallel over models "
+                         "(oracle/lcurve_oracle.cpp, FP64 restatement of the reference CPU path)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 eclipses + f32 flux", "data": "synthetic",
+        "config": {"workload": f"batch_{args.models}: uneven models (nlat1f U{{30..300}}, nlat2f U{{30..500}}, "
+                               f"ntime U{{200..5000}}, q/iangle/r1/t1/t2 uniform), seed 1234+rank",
+                   "models_per_gpu": args.models, "elements_per_step": st["elements"],
+                   "subphases_per_step": st["subphases"], "element_evals_per_step": st["element_evals"],
+                   "roche_eclipsed_elements": st["roche_elements"], "roche_search": counts,
+                   "flux_units": st["flux_units"],
+                   "stage_ms": dict(zip(stage_names, [float(x) for x in stage])),
+                   "l2": "inputs larger than L2 (element arrays > 10 GB per step)",
+                   "parallelism": f"weak, {world} independent batches"},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": 6 * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

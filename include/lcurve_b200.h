@@ -119,6 +119,17 @@ void lcb_free_data(lcb_datum* data);
 int lcb_light_curve(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
                     int scale, int rdata, double* calc_out, lcb_result* res_out);
 
+/* ---- grid inspection --------------------------------------------------------
+ * The elements the GPU builds for one model -- the grids of set_star_grid /
+ * set_disc_grid / set_disc_edge / set_bright_spot_grid after continuum and
+ * eclipses (grid.rs, brightness.rs; the reference inspects them in
+ * crates/lcurve/examples/diag.rs).  which: 0 star1 fine, 1 star2 fine,
+ * 2 star1 coarse, 3 star2 coarse, 4 disc, 5 rim, 6 bright spot.  Call with
+ * NULL arrays to get *n; then posn/dirn hold 3n doubles, area/gravity/flux n
+ * floats and ecl 8n doubles: four (ingress, egress) pairs, unused = (+inf, -inf). */
+int lcb_model_grid(lcb_ctx* ctx, const lcb_model* model, int which, int64_t* n, double* posn, double* dirn,
+                   float* area, float* gravity, float* flux, double* ecl);
+
 /* ---- batched chi-squared ---------------------------------------------------
  * chisq_batch(base, data, names, values, scale) (orchestration.rs:329-357)
  * and chisq_batch_gpu (crates/lcurve-cuda/src/batch.rs:73-80): values is an
@@ -150,11 +161,30 @@ int  lcb_batch_set_params(lcb_batch* b, const char* const* names, int ndim, cons
 int  lcb_batch_run(lcb_batch* b, int scale);
 int  lcb_batch_results(lcb_batch* b, double* chisq_out, double* calc_out, lcb_result* res_out);
 /* Work counts of the planned batch: [models, elements, sub-phases,
- * element-evals, flux work units, roche-eclipsed elements, pad, pad]. */
+ * element-evals, flux work units, roche-eclipsed elements, Roche potential
+ * evaluations and gradient evaluations of the eclipse search in the last run]. */
 int  lcb_batch_stats(const lcb_batch* b, int64_t* out8);
-/* Device time (ms) of each stage of the last lcb_batch_run, measured with
- * CUDA events on the launching stream: [phase, elements, flux, epilogue]. */
-int  lcb_batch_stage_ms(const lcb_batch* b, double* out4);
+/* Eclipse-search counters of the last run: [potential evaluations, gradient
+ * evaluations, line-of-sight searches, lower-bound nodes, searches proven to
+ * miss by the lower bound and skipped]. */
+int  lcb_batch_search_counts(const lcb_batch* b, int64_t* out5);
+/* Same evaluation as lcb_batch_run but issued as direct launches with CUDA
+ * events between the stages (events recorded inside a graph carry no timing),
+ * for per-kernel device times. */
+int  lcb_batch_profile(lcb_batch* b, int scale);
+/* Device time (ms) of each stage of the last lcb_batch_profile, measured with
+ * CUDA events on the launching stream: [phase, elements (grid + continuum +
+ * analytic eclipses), roche (FP64 ray-march), aux (per-model sums), flux,
+ * epilogue]. */
+int  lcb_batch_stage_ms(const lcb_batch* b, double* out6);
+
+/* ---- measurement utilities (no reference counterpart) --------------------
+ * Bytes the last call on this context copied host->device / device->host. */
+int lcb_ctx_transfer_bytes(const lcb_ctx* ctx, int64_t* h2d, int64_t* d2h);
+/* FMA throughput of the context's device in TFLOP/s, measured with a CUDA
+ * kernel of independent FMA chains: which = 0 FP32, 1 FP64.  These are the
+ * roofline denominators of the FP32 flux kernel and the FP64 eclipse kernel. */
+int lcb_measure_fma_peak(lcb_ctx* ctx, int which, double* tflops);
 
 #ifdef __cplusplus
 }

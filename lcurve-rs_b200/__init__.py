@@ -82,6 +82,25 @@ def _ctx() -> C.c_void_p:
         return h
 
 
+def transfer_bytes() -> tuple[int, int]:
+    """(host->device, device->host) bytes of the last call on the current device's context."""
+    h, d = C.c_int64(), C.c_int64()
+    check(_capi.load().lcb_ctx_transfer_bytes(_ctx(), C.byref(h), C.byref(d)))
+    return h.value, d.value
+
+
+def fma_peak_tflops(fp64: bool) -> float:
+    """Measured FMA throughput of the current device (TFLOP/s)."""
+    v = C.c_double()
+    check(_capi.load().lcb_measure_fma_peak(_ctx(), int(bool(fp64)), C.byref(v)))
+    return v.value
+
+
+def set_stream(cuda_stream: int) -> None:
+    """Issue this device's work on an existing cudaStream_t (e.g. a torch stream's cuda_stream)."""
+    check(_capi.load().lcb_ctx_set_stream(_ctx(), C.c_void_p(cuda_stream)))
+
+
 def make_data(times, expose=0.001, ndiv=1, flux=0.0, ferr=1.0, weight=1.0) -> np.ndarray:
     """Structured array of lcb_datum records."""
     times = np.atleast_1d(np.asarray(times, dtype=np.float64))
@@ -283,6 +302,23 @@ class Model:
                                            dptr(values), nsets, int(bool(scale)), dptr(out)))
         return out
 
+    GRIDS = {"star1f": 0, "star2f": 1, "star1c": 2, "star2c": 3, "disc": 4, "edge": 5, "spot": 6}
+
+    def grid(self, which: str) -> dict:
+        """Elements of one grid as built on the GPU (posn, dirn, area, gravity, flux, ecl pairs)."""
+        L = _capi.load()
+        w = self.GRIDS[which]
+        n = C.c_int64()
+        check(L.lcb_model_grid(_ctx(), self._h, w, C.byref(n), None, None, None, None, None, None))
+        k = n.value
+        posn, dirn, ecl = np.zeros((k, 3)), np.zeros((k, 3)), np.zeros((k, 8))
+        area, grav, flux = np.zeros(k, np.float32), np.zeros(k, np.float32), np.zeros(k, np.float32)
+        fp = C.POINTER(C.c_float)
+        if k:
+            check(L.lcb_model_grid(_ctx(), self._h, w, C.byref(n), dptr(posn), dptr(dirn), area.ctypes.data_as(fp),
+                                   grav.ctypes.data_as(fp), flux.ctypes.data_as(fp), dptr(ecl)))
+        return dict(posn=posn, dirn=dirn, area=area, gravity=grav, flux=flux, ecl=ecl)
+
     def __repr__(self):
         return (f"Model(q={self.q}, iangle={self.iangle}, r1={self.r1}, r2={self.r2}, t1={self.t1}, "
                 f"t2={self.t2})")
@@ -329,6 +365,17 @@ class Batch:
     def run(self, scale=False) -> None:
         check(_capi.load().lcb_batch_run(self._h, int(bool(scale))))
 
+    def search_counts(self) -> dict:
+        a = np.zeros(5, dtype=np.int64)
+        check(_capi.load().lcb_batch_search_counts(self._h, i64ptr(a)))
+        return dict(pot_evals=int(a[0]), dpot_evals=int(a[1]), searches=int(a[2]), bound_nodes=int(a[3]),
+                    proven_misses=int(a[4]))
+
+    def profile(self, scale=False) -> dict:
+        """Run once with direct launches and CUDA events between stages; returns stage_ms()."""
+        check(_capi.load().lcb_batch_profile(self._h, int(bool(scale))))
+        return self.stage_ms()
+
     def results(self, want_calc=False):
         chisq = np.zeros(self.n)
         calc = np.zeros(self._data.shape[0]) if want_calc else None
@@ -340,9 +387,9 @@ class Batch:
         a = np.zeros(8, dtype=np.int64)
         check(_capi.load().lcb_batch_stats(self._h, i64ptr(a)))
         return dict(models=int(a[0]), elements=int(a[1]), subphases=int(a[2]), element_evals=int(a[3]),
-                    flux_units=int(a[4]), roche_elements=int(a[5]))
+                    flux_units=int(a[4]), roche_elements=int(a[5]), pot_evals=int(a[6]), dpot_evals=int(a[7]))
 
     def stage_ms(self) -> dict:
-        a = np.zeros(4)
+        a = np.zeros(6)
         check(_capi.load().lcb_batch_stage_ms(self._h, dptr(a)))
-        return dict(phase=a[0], elements=a[1], flux=a[2], epilogue=a[3])
+        return dict(phase=a[0], elements=a[1], roche=a[2], aux=a[3], flux=a[4], epilogue=a[5])

@@ -43,7 +43,8 @@ SYMBOLS = [
     "lcb_model_set_param", "lcb_model_get_param", "lcb_model_get_pparam", "lcb_model_set_pparam",
     "lcb_model_set_comp", "lcb_model_get_comp", "lcb_param_name", "lcb_read_data", "lcb_free_data",
     "lcb_light_curve", "lcb_chisq_batch", "lcb_chisq_batch_ragged", "lcb_batch_create", "lcb_batch_destroy",
-    "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_stage_ms",
+    "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_profile", "lcb_batch_stage_ms",
+    "lcb_ctx_transfer_bytes", "lcb_measure_fma_peak", "lcb_model_grid", "lcb_batch_search_counts",
 ]
 
 _lib = None
@@ -80,7 +81,13 @@ def load():
         "lcb_batch_run": ([vp, i], i),
         "lcb_batch_results": ([vp, dp, dp, C.POINTER(Result)], i),
         "lcb_batch_stats": ([vp, i64p], i),
+        "lcb_batch_profile": ([vp, i], i),
         "lcb_batch_stage_ms": ([vp, dp], i),
+        "lcb_ctx_transfer_bytes": ([vp, i64p, i64p], i),
+        "lcb_measure_fma_peak": ([vp, i, dp], i),
+        "lcb_model_grid": ([vp, vp, i, i64p, dp, dp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                            C.POINTER(C.c_float), dp], i),
+        "lcb_batch_search_counts": ([vp, i64p], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -59,12 +59,13 @@ struct DevBuf {
 
 // All device storage of one planned batch.
 struct DeviceSet {
-    DevBuf models, segs, bands, rings, eblocks, units, dmodel, dsub0, dsrc, data;
-    DevBuf rec, pos, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter, datum;
+    DevBuf models, segs, bands, rings, eblocks, rblocks, ablocks, units, dmodel, dsub0, dsrc, data;
+    DevBuf rec, pos, p64, d64, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter,
+        datum, ecount;
     void release() {
-        for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &units, &dmodel, &dsub0, &dsrc, &data, &rec, &pos,
-                          &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac, &partial, &calc, &results, &counter,
-                          &datum})
+        for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &rblocks, &ablocks, &units, &dmodel, &dsub0, &dsrc,
+                          &data, &rec, &pos, &p64, &d64, &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac,
+                          &partial, &calc, &results, &counter, &datum, &ecount})
             b->release();
     }
 };
@@ -75,6 +76,8 @@ struct lcb_model {
     lcb::Model m;
 };
 
+constexpr int kStages = 6;  // phase, elements, roche, aux, flux, epilogue
+
 struct lcb_ctx {
     int device = 0;
     int num_sms = 148;
@@ -83,7 +86,8 @@ struct lcb_ctx {
     std::mutex mu;
     std::string last_error;
     DeviceSet scratch;  // buffers of transient (non-resident) calls
-    cudaEvent_t ev[5] = {};
+    cudaEvent_t ev[kStages + 1] = {};
+    int64_t h2d = 0, d2h = 0;  // bytes moved by the current / last call
 };
 
 struct lcb_batch {
@@ -97,9 +101,10 @@ struct lcb_batch {
     int graph_scale = -1;
     std::vector<int64_t> graph_key;
     bool ran = false;
-    double stage_ms[4] = {0, 0, 0, 0};
+    double stage_ms[kStages] = {0, 0, 0, 0, 0, 0};
     std::vector<double> h_results, h_calc;
     std::vector<int> h_status;
+    unsigned long long ecount[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -111,6 +116,7 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     auto put = [&](DevBuf& b, const void* src, size_t bytes) {
         b.ensure(bytes);
         if (bytes) CUDA_TRY(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
+        C->h2d += (int64_t)bytes;
     };
     const int64_t nm = (int64_t)P.models.size();
     put(D.models, P.models.data(), nm * sizeof(lcb::ModelDev));
@@ -118,6 +124,8 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     put(D.bands, P.bands.data(), P.bands.size() * sizeof(lcb::Band));
     put(D.rings, P.rings.data(), P.rings.size() * sizeof(lcb::Ring));
     put(D.eblocks, P.eblocks.data(), P.eblocks.size() * sizeof(lcb::ElemBlock));
+    put(D.rblocks, P.rblocks.data(), P.rblocks.size() * sizeof(lcb::ElemBlock));
+    put(D.ablocks, P.ablocks.data(), P.ablocks.size() * sizeof(lcb::ElemBlock));
     put(D.units, P.units.data(), P.units.size() * sizeof(lcb::FluxUnit));
     put(D.dmodel, P.datum_model.data(), P.datum_model.size() * sizeof(int32_t));
     put(D.dsub0, P.datum_sub0.data(), P.datum_sub0.size() * sizeof(int64_t));
@@ -130,6 +138,8 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     }
     D.rec.ensure(P.nelem * sizeof(float4));
     D.pos.ensure(P.nelem * sizeof(float4));
+    D.p64.ensure(P.nelem * sizeof(double4));
+    D.d64.ensure(P.nelem * sizeof(double4));
     D.ecl.ensure(P.nelem * lcb::kMaxEcl * sizeof(double2));
     D.aux.ensure(nm * lcb::kNumAux * sizeof(double));
     D.status.ensure(nm * sizeof(int));
@@ -142,6 +152,7 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     D.calc.ensure(P.ndatum * sizeof(double));
     D.results.ensure(nm * 12 * sizeof(double));
     D.counter.ensure(sizeof(int) * 4);
+    D.ecount.ensure(sizeof(unsigned long long) * 8);
 }
 
 // The device launch sequence of one batch evaluation.
@@ -151,6 +162,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     CUDA_TRY(cudaMemsetAsync(D.aux.p, 0, nm * lcb::kNumAux * sizeof(double), s));
     CUDA_TRY(cudaMemsetAsync(D.status.p, 0, nm * sizeof(int), s));
     CUDA_TRY(cudaMemsetAsync(D.counter.p, 0, sizeof(int) * 4, s));
+    CUDA_TRY(cudaMemsetAsync(D.ecount.p, 0, sizeof(unsigned long long) * 8, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[0], s));
     lcb::PhaseArgs pa{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dmodel.as<int32_t>(),
                       D.dsub0.as<int64_t>(), P.ndatum, D.spe.as<float4>(), D.spphi.as<double>(),
@@ -158,10 +170,17 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     CUDA_TRY(lcb::launch_phase(pa, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[1], s));
     lcb::ElemArgs ea{D.models.as<lcb::ModelDev>(), D.segs.as<lcb::SegDesc>(), D.eblocks.as<lcb::ElemBlock>(),
-                     D.bands.as<lcb::Band>(), D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(),
-                     D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(), (int64_t)P.eblocks.size()};
+                     D.rblocks.as<lcb::ElemBlock>(), D.ablocks.as<lcb::ElemBlock>(), D.bands.as<lcb::Band>(),
+                     D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
+                     D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
+                     (int64_t)P.eblocks.size(), (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(),
+                     D.ecount.as<unsigned long long>()};
     CUDA_TRY(lcb::launch_elements(ea, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[2], s));
+    CUDA_TRY(lcb::launch_roche(ea, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[3], s));
+    CUDA_TRY(lcb::launch_aux(ea, s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[4], s));
     lcb::FluxArgs fa{D.models.as<lcb::ModelDev>(), D.units.as<lcb::FluxUnit>(), (int64_t)P.units.size(),
                      D.counter.as<int>(), D.rec.as<float4>(), D.pos.as<float4>(), D.ecl.as<double2>(),
                      D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
@@ -169,13 +188,13 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     int64_t grid = (int64_t)C->num_sms * lcb::flux_blocks_per_sm();
     grid = std::min<int64_t>(grid, std::max<int64_t>((int64_t)P.units.size(), 1));
     CUDA_TRY(lcb::launch_flux(fa, (int)grid, s));
-    if (timed) CUDA_TRY(cudaEventRecord(C->ev[3], s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[5], s));
     lcb::EpiArgs pe{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dsub0.as<int64_t>(),
                     D.spphi.as<double>(), D.spw.as<double>(), D.slfac.as<double>(), D.partial.as<double>(),
                     D.aux.as<double>(), D.status.as<int>(), scale, rdata, D.calc.as<double>(),
                     D.results.as<double>(), nm};
     CUDA_TRY(lcb::launch_epilogue(pe, s));
-    if (timed) CUDA_TRY(cudaEventRecord(C->ev[4], s));
+    if (timed) CUDA_TRY(cudaEventRecord(C->ev[6], s));
 }
 
 void set_device(lcb_ctx* C) { CUDA_TRY(cudaSetDevice(C->device)); }
@@ -194,6 +213,8 @@ void fetch_results(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, std::vector<dou
         status->resize(nm);
         CUDA_TRY(cudaMemcpyAsync(status->data(), D.status.p, nm * sizeof(int), cudaMemcpyDeviceToHost, C->stream));
     }
+    C->d2h += (int64_t)(nm * 12 * sizeof(double)) + (calc ? P.ndatum * (int64_t)sizeof(double) : 0) +
+              (status ? nm * (int64_t)sizeof(int) : 0);
     CUDA_TRY(cudaStreamSynchronize(C->stream));
 }
 
@@ -226,6 +247,8 @@ int guarded(lcb_ctx* C, F&& f) {
         if (C) {
             std::lock_guard<std::mutex> g(C->mu);
             set_device(C);
+            (void)cudaGetLastError();  // a stale non-sticky error must not be blamed on this call
+            C->h2d = C->d2h = 0;
             f();
         } else {
             f();
@@ -414,6 +437,62 @@ int lcb_light_curve(lcb_ctx* C, const lcb_model* model, const lcb_datum* data, i
     });
 }
 
+int lcb_model_grid(lcb_ctx* C, const lcb_model* model, int which, int64_t* n, double* posn, double* dirn,
+                   float* area, float* gravity, float* flux, double* ecl) {
+    if (!C || !model || !n || which < 0 || which > 6) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] {
+        const lcb::Model* mp = &model->m;
+        lcb_datum d{};
+        d.time = 0.0; d.expose = 0.0; d.ferr = 1.0; d.weight = 1.0; d.ndiv = 1;
+        int64_t st = 0, cnt = 1;
+        lcb::Plan P;
+        lcb::plan_batch(&mp, 1, &d, &st, &cnt, C->num_sms, P);
+        if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
+        const lcb::SegDesc* g = nullptr;
+        for (const auto& sg : P.segs) {
+            bool star = sg.kind == lcb::SEG_STAR1 || sg.kind == lcb::SEG_STAR2;
+            int k = sg.kind == lcb::SEG_STAR1 ? 1 : 2;
+            if (star && which <= 3) {
+                bool fine = which <= 1;
+                if ((which % 2 == 0 ? 1 : 2) != k) continue;
+                if (sg.role == lcb::ROLE_BOTH || (sg.role == lcb::ROLE_FINE) == fine) { g = &sg; break; }
+            } else if ((which == 4 && sg.kind == lcb::SEG_DISC) || (which == 5 && sg.kind == lcb::SEG_EDGE) ||
+                       (which == 6 && sg.kind == lcb::SEG_SPOT)) {
+                g = &sg;
+                break;
+            }
+        }
+        *n = g ? g->count : 0;
+        if (!g || !posn) return;
+        upload_plan(C, C->scratch, P, &d, 1, true);
+        enqueue_run(C, C->scratch, P, 0, 0, false);
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+        std::vector<double4> p64(g->count), d64(g->count);
+        std::vector<float4> rec(g->count);
+        std::vector<double2> e(g->count * lcb::kMaxEcl);
+        CUDA_TRY(cudaMemcpy(p64.data(), C->scratch.p64.as<double4>() + g->first, g->count * sizeof(double4),
+                            cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(d64.data(), C->scratch.d64.as<double4>() + g->first, g->count * sizeof(double4),
+                            cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(rec.data(), C->scratch.rec.as<float4>() + g->first, g->count * sizeof(float4),
+                            cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(e.data(), C->scratch.ecl.as<double2>() + g->first * lcb::kMaxEcl,
+                            e.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < g->count; ++i) {
+            posn[3 * i] = p64[i].x; posn[3 * i + 1] = p64[i].y; posn[3 * i + 2] = p64[i].z;
+            if (dirn) { dirn[3 * i] = d64[i].x; dirn[3 * i + 1] = d64[i].y; dirn[3 * i + 2] = d64[i].z; }
+            if (area) area[i] = (float)p64[i].w;
+            if (gravity) gravity[i] = (float)d64[i].w;
+            if (flux) flux[i] = rec[i].w;
+            if (ecl)
+                for (int k = 0; k < lcb::kMaxEcl; ++k) {
+                    ecl[8 * i + 2 * k] = e[i * lcb::kMaxEcl + k].x;
+                    ecl[8 * i + 2 * k + 1] = e[i * lcb::kMaxEcl + k].y;
+                }
+        }
+    });
+}
+
 int lcb_chisq_batch(lcb_ctx* C, const lcb_model* base, const lcb_datum* data, int64_t n, const char* const* names,
                     int ndim, const double* values, int64_t nsets, int scale, double* chisq_out) {
     if (!C || !base || !data || !names || !values || !chisq_out) return fail(LCB_ERR_INVALID, "null pointer");
@@ -559,7 +638,7 @@ int lcb_batch_run(lcb_batch* B, int scale) {
             cudaGraph_t g;
             CUDA_TRY(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                enqueue_run(C, B->dev, B->plan, scale, 1, true);
+                enqueue_run(C, B->dev, B->plan, scale, 1, false);
             } catch (...) {
                 cudaStreamEndCapture(C->stream, &g);
                 throw;
@@ -573,9 +652,24 @@ int lcb_batch_run(lcb_batch* B, int scale) {
         }
         CUDA_TRY(cudaGraphLaunch(B->graph, C->stream));
         fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
-        for (int k = 0; k < 4; ++k) {
+        CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
+        B->ran = true;
+        for (int s : B->h_status)
+            if (s & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+    });
+}
+
+int lcb_batch_profile(lcb_batch* B, int scale) {
+    if (!B) return fail(LCB_ERR_INVALID, "null batch");
+    lcb_ctx* C = B->ctx;
+    return guarded(C, [&] {
+        enqueue_run(C, B->dev, B->plan, scale, 1, true);
+        fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
+        CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < kStages; ++k) {
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, C->ev[k], C->ev[k + 1]) == cudaSuccess) B->stage_ms[k] = ms;
+            CUDA_TRY(cudaEventElapsedTime(&ms, C->ev[k], C->ev[k + 1]));
+            B->stage_ms[k] = ms;
         }
         B->ran = true;
         for (int s : B->h_status)
@@ -607,15 +701,34 @@ int lcb_batch_results(lcb_batch* B, double* chisq_out, double* calc_out, lcb_res
 int lcb_batch_stats(const lcb_batch* B, int64_t* out8) {
     if (!B || !out8) return fail(LCB_ERR_INVALID, "null pointer");
     const lcb::Plan& P = B->plan;
-    int64_t v[8] = {(int64_t)P.models.size(), P.nelem, P.nsub, P.evals, (int64_t)P.units.size(), P.roche_elems, 0, 0};
+    int64_t v[8] = {(int64_t)P.models.size(), P.nelem, P.nsub, P.evals, (int64_t)P.units.size(), P.roche_elems,
+                    (int64_t)B->ecount[0], (int64_t)B->ecount[1]};
     std::memcpy(out8, v, sizeof v);
     return LCB_OK;
 }
 
-int lcb_batch_stage_ms(const lcb_batch* B, double* out4) {
-    if (!B || !out4) return fail(LCB_ERR_INVALID, "null pointer");
-    for (int k = 0; k < 4; ++k) out4[k] = B->stage_ms[k];
+int lcb_batch_search_counts(const lcb_batch* B, int64_t* out5) {
+    if (!B || !out5) return fail(LCB_ERR_INVALID, "null pointer");
+    for (int k = 0; k < 5; ++k) out5[k] = (int64_t)B->ecount[k];
     return LCB_OK;
+}
+
+int lcb_batch_stage_ms(const lcb_batch* B, double* out6) {
+    if (!B || !out6) return fail(LCB_ERR_INVALID, "null pointer");
+    for (int k = 0; k < kStages; ++k) out6[k] = B->stage_ms[k];
+    return LCB_OK;
+}
+
+int lcb_ctx_transfer_bytes(const lcb_ctx* C, int64_t* h2d, int64_t* d2h) {
+    if (!C || !h2d || !d2h) return fail(LCB_ERR_INVALID, "null pointer");
+    *h2d = C->h2d;
+    *d2h = C->d2h;
+    return LCB_OK;
+}
+
+int lcb_measure_fma_peak(lcb_ctx* C, int which, double* tflops) {
+    if (!C || !tflops || (which != 0 && which != 1)) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] { CUDA_TRY(lcb::measure_fma_peak(which, C->num_sms, C->stream, tflops)); });
 }
 
 }  // extern "C"

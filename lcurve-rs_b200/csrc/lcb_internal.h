@@ -128,9 +128,9 @@ struct Ring {               // one disc annulus (grid.rs:356-364)
     double rad, h, cosp, sinp, area;
 };
 
-struct ElemBlock {          // one 256-element block of the element kernel
+struct ElemBlock {          // one block of an element kernel
     int32_t seg;
-    int32_t pad;
+    int32_t by;             // k_roche: eclipsing star (1 or 2)
     int64_t offset;         // element offset within the segment
 };
 
@@ -160,6 +160,7 @@ constexpr int kFluxR = 4;                          // sub-phases per thread
 constexpr int kFluxTile = kFluxThreads * kFluxR;   // sub-phases per work unit
 constexpr int kFluxChunk = 256;                    // elements staged per TMA chunk
 constexpr int kElemThreads = 256;
+constexpr int kRocheBlock = 128;                   // elements per k_roche block
 
 // Device status bits (ModelDev.status / batch status word).
 constexpr int kStatusIterCap = 1;     // an iteration cap without a reference counterpart tripped

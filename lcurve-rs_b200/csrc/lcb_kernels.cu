@@ -22,6 +22,7 @@
 //   k_epilogue : one block per model: ginterp scale factors, exposure
 //                smearing, slope/third, chi-squared / re_scale
 //                (orchestration.rs:243-310, 361-401).
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -38,6 +39,8 @@ constexpr double kFac2 = 1.0e9 * 6.6262e-34 * 2.99792458e8 / 1.3806e-23;  // pla
 constexpr double kFwhmEfac = 2.3548200450309493;                  // brightness.rs:8
 constexpr double kEfac = 1.0000001;                               // grid.rs:396
 constexpr int kFblinkEvalCap = 1 << 18;  // bound on one line-of-sight search (reference has none)
+constexpr int kRocheMinBlocks = 4;
+constexpr int kCertBudget = 32;   // lower-bound nodes per line of sight before the full search
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 __device__ __forceinline__ double rad2deg(double r) { return r * (180.0 / kPi); }
@@ -97,16 +100,22 @@ __device__ __forceinline__ double los_dpot(const RocheEcl& s, const Los& L, doub
     return gx * L.ex + gy * L.ey + gz * L.ez;
 }
 
+// Work counters of the eclipse search (potential and gradient evaluations, fblink calls).
+struct EclCount {
+    int pot = 0, dpot = 0, fbl = 0, cert = 0, skipped = 0;
+};
+
 // dbrent with stop-fast (crates/subs/src/numerical/dbrent.rs:20-165).
-// Returns 1 = bracketed minimum below fref, 0 = not below, and uses *evals.
+// Returns 1 = bracketed minimum below fref, 0 = not below.
 __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double bx, double cx, double acc,
-                             double fref, int& evals) {
+                             double fref, EclCount& cnt) {
     double a = fmin(ax, cx), b = fmax(ax, cx);
     double x = bx, w = bx, v = bx;
     double fx = los_pot(s, L, x), fw = fx, fv = fx;
-    ++evals;
+    ++cnt.pot;
     if (fx < fref) return true;
     double dx = los_dpot(s, L, x), dw = dx, dv = dx;
+    ++cnt.dpot;
     double e = 0.0, d = 0.0;
     for (int it = 0; it < 100; ++it) {
         double xm = 0.5 * (a + b);
@@ -142,16 +151,17 @@ __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double 
         if (fabs(d) >= tol1) {
             u = x + d;
             fu = los_pot(s, L, u);
-            ++evals;
+            ++cnt.pot;
             if (fu < fref) return true;
         } else {
             u = x + (d >= 0.0 ? fabs(tol1) : -fabs(tol1));
             fu = los_pot(s, L, u);
-            ++evals;
+            ++cnt.pot;
             if (fu < fref) return true;
             if (fu > fx) return fx < fref;
         }
         double du = los_dpot(s, L, u);
+        ++cnt.dpot;
         if (fu <= fx) {
             if (u >= x) a = x; else b = x;
             v = w; fv = fw; dv = dw;
@@ -170,8 +180,65 @@ __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double 
     return false;  // iteration cap: the reference maps its Err to "not eclipsed"
 }
 
+// Rigorous lower bound of the Roche potential on the segment p + lam*e,
+// lam in [a, b] (|e| = 1): the two gravity terms are bounded at the closest
+// approach to each star, the centrifugal term (convex along a line) and the
+// linear term at the end points.
+__device__ __forceinline__ double pot_lower_bound(const RocheEcl& s, const Los& L, double a, double b) {
+    // distance to the primary (origin)
+    double t1 = fmin(fmax(-(L.px * L.ex + L.py * L.ey + L.pz * L.ez), a), b);
+    double x1 = fma(t1, L.ex, L.px), y1 = fma(t1, L.ey, L.py), z1 = fma(t1, L.ez, L.pz);
+    double d1 = x1 * x1 + y1 * y1 + z1 * z1;
+    // distance to the secondary (1, 0, 0)
+    double qx = L.px - 1.0;
+    double t2 = fmin(fmax(-(qx * L.ex + L.py * L.ey + L.pz * L.ez), a), b);
+    double x2 = fma(t2, L.ex, qx), y2 = fma(t2, L.ey, L.py), z2 = fma(t2, L.ez, L.pz);
+    double d2 = x2 * x2 + y2 * y2 + z2 * z2;
+    double xa = fma(a, L.ex, L.px), ya = fma(a, L.ey, L.py);
+    double xb = fma(b, L.ex, L.px), yb = fma(b, L.ey, L.py);
+    double lb = -s.comp * rsqrt(d1) - s.mu * rsqrt(d2);
+    // the rest is a concave quadratic along the line: its minimum is at an end point
+    if (s.primary) {  // rpot1: - ssq (x^2+y^2)/2 + mu x
+        double ca = -0.5 * s.ssq * (xa * xa + ya * ya) + s.mu * xa;
+        double cb = -0.5 * s.ssq * (xb * xb + yb * yb) + s.mu * xb;
+        return lb + fmin(ca, cb);
+    }
+    // rpot2: - ssq ((x-1)^2 + y^2)/2 - comp x
+    double ca = -0.5 * s.ssq * ((xa - 1.0) * (xa - 1.0) + ya * ya) - s.comp * xa;
+    double cb = -0.5 * s.ssq * ((xb - 1.0) * (xb - 1.0) + yb * yb) - s.comp * xb;
+    return lb + fmin(ca, cb);
+}
+
+// True when the potential provably stays above the surface value on the whole
+// line-of-sight segment [a, b]: an adaptive march over sub-segments, each
+// certified by pot_lower_bound with a margin of 1e-9 relative (far above the
+// rounding of any potential evaluation).  False means "not proven".
+__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int& nodes) {
+    const double thr = s.pref + 1e-9 * fmax(fabs(s.pref), 1.0);
+    const double hmin = 1e-6 * (b - a);
+    double t = a, h = b - a;
+    for (int it = 0; it < kCertBudget; ++it) {
+        if (t >= b) return true;
+        double hh = fmin(h, b - t);
+        ++nodes;
+        if (pot_lower_bound(s, L, t, t + hh) > thr) {
+            t += hh;
+            h = 2.0 * hh;
+        } else {
+            if (hh <= hmin) return false;
+            h = 0.5 * hh;
+        }
+    }
+    return t >= b;
+}
+
 // Is point p hidden from earth direction e by the Roche star? (eclipse.rs:123-197)
-__device__ bool fblink(const RocheEcl& s, double acc, const Los& L, int& evals, bool& capped) {
+// With `prove` set, a line of sight whose first reference evaluation is not
+// inside the star is first tested with the rigorous lower bound: every point
+// the reference search evaluates lies in [lam1 - acc, lam2 + acc] (dbrent.rs:116
+// may step acc past an end), so a proven miss is exactly its "false".
+__device__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, bool prove) {
+    ++cnt.fbl;
     double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
     double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
     if (bq >= 0.0) return false;
@@ -182,26 +249,40 @@ __device__ bool fblink(const RocheEcl& s, double acc, const Los& L, int& evals, 
     double lam2 = -bq + fac, lam1 = fmax(cq / lam2, 0.0);
     if (lam1 == 0.0) return true;
     const double pref = s.pref;
-    int nstep = 1;
-    double step = lam2 - lam1, f1 = 0.0, f2 = 0.0, flam = 1.0, lam = lam1;
-    int local = 0;
-    while (step > acc) {
-        lam = lam1 + step / 2.0;
-        bool br = false;
-        for (int n = 0; n < nstep; ++n) {
-            flam = los_pot(s, L, lam + (double)n * step);
-            ++local;
-            if (flam <= pref) { evals += local; return true; }
-            if (nstep == 1) { f1 = los_pot(s, L, lam1); f2 = los_pot(s, L, lam2); local += 2; }
-            if (flam < f1 && flam < f2) { lam = lam + (double)n * step; br = true; break; }
-        }
-        if (br) break;
-        if (local > kFblinkEvalCap) { capped = true; evals += local; return false; }
-        step /= 2.0;
-        nstep *= 2;
+    double step = lam2 - lam1;
+    if (!(step > acc)) return false;  // no evaluation: flam = 1 > f1 = f2 = 0
+    // the reference's first evaluation, at the middle of the chord
+    const double lam0 = lam1 + step / 2.0;
+    double flam = los_pot(s, L, lam0);
+    ++cnt.pot;
+    if (flam <= pref) return true;
+    if (prove) {
+        const double pad = 1.001 * acc + 1e-12;
+        if (certify_miss(s, L, lam1 - pad, lam2 + pad, cnt.cert)) { ++cnt.skipped; return false; }
     }
-    evals += local;
-    if (flam < f1 && flam < f2) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, evals);
+    int nstep = 1;
+    double f1 = los_pot(s, L, lam1), f2 = los_pot(s, L, lam2), lam = lam0;
+    int local = 2;
+    bool br = flam < f1 && flam < f2;
+    if (!br) {
+        step /= 2.0;
+        nstep = 2;
+        while (step > acc) {
+            lam = lam1 + step / 2.0;
+            for (int n = 0; n < nstep; ++n) {
+                flam = los_pot(s, L, lam + (double)n * step);
+                ++local;
+                if (flam <= pref) { cnt.pot += local; return true; }
+                if (flam < f1 && flam < f2) { lam = lam + (double)n * step; br = true; break; }
+            }
+            if (br) break;
+            if (local > kFblinkEvalCap) { capped = true; cnt.pot += local; return false; }
+            step /= 2.0;
+            nstep *= 2;
+        }
+    }
+    cnt.pot += local;
+    if (br) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, cnt);
     return false;
 }
 
@@ -242,12 +323,11 @@ __device__ bool sphere_phase(double cosi, double sini, double px, double py, dou
 
 // Ingress/egress of point p behind a Roche-distorted star (eclipse.rs:270-373).
 __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
-                               double pz, double& ing, double& eg, bool& capped) {
+                               double pz, double& ing, double& eg, bool& capped, EclCount& evals) {
     double phi1, phi2, lam1, lam2;
     if (!sphere_phase(cosi, sini, px, py, pz, s.cofmx, s.rref, phi1, phi2, lam1, lam2)) return false;
     double acc = 2.0 * sqrt(2.0 * kTwoPi * (lam2 - lam1) * delta);
     Los L{px, py, pz, 0.0, 0.0, 0.0};
-    int evals = 0;
     // pot_min_search: first scanned phase that is eclipsed (eclipse.rs:347-373)
     double ns = ceil((phi2 - phi1) / (acc / kTwoPi));
     int nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
@@ -257,7 +337,7 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
     for (int i = 0; i <= nsteps; ++i) {
         phi = phi1 + (double)i * dphi;
         earth_at(cosi, sini, phi, L.ex, L.ey, L.ez);
-        if (fblink(s, acc, L, evals, capped)) { found = true; break; }
+        if (fblink(s, acc, L, evals, capped, true)) { found = true; break; }
         if (capped) return false;
     }
     if (!found) return false;
@@ -265,7 +345,7 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
         for (int it = 0; it < 200 && fabs(pin - pout) > delta; ++it) {
             double pmid = (pin + pout) / 2.0;
             earth_at(cosi, sini, pmid, L.ex, L.ey, L.ez);
-            if (fblink(s, acc, L, evals, capped)) pin = pmid; else pout = pmid;
+            if (fblink(s, acc, L, evals, capped, false)) pin = pmid; else pout = pmid;
         }
         return (pin + pout) / 2.0;
     };
@@ -425,211 +505,262 @@ __device__ __forceinline__ double lens_mag_d(double sx, double sy, double sz, do
 }
 
 // ---------------------------------------------------------------------------
-// k_elements
+// k_elements: grid, continuum, analytic eclipses
 // ---------------------------------------------------------------------------
+// Eclipse pair slots per element: star elements use slot 0 for the eclipse by
+// the other star and slots 1-2 for the opaque disc; disc, rim and spot
+// elements use slots 0-1 for the disc, 2 for star 1 and 3 for star 2.  A
+// Roche-distorted eclipser leaves its slot empty here for k_roche to fill.
+__device__ __forceinline__ int roche_slot(int kind, int by) {
+    return (kind == SEG_STAR1 || kind == SEG_STAR2) ? 0 : (by == 1 ? 2 : 3);
+}
+
 __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
     const ElemBlock blk = A.blocks[blockIdx.x];
     const SegDesc sg = A.segs[blk.seg];
     const ModelDev& M = A.models[sg.model];
     const int64_t i = blk.offset + threadIdx.x;
-    const bool valid = i < sg.count;
+    if (i >= sg.count) return;
 
     double px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 1;
     float area = 0.f, grav = 1.f, flux = 0.f;
-    double ing[kMaxEcl], eg[kMaxEcl];
-    int necl = 0, nse = 0;  // total pairs; pairs from the star eclipse (before disc pairs)
-    bool capped = false;
+    double2 ecl[kMaxEcl];
+    for (int k = 0; k < kMaxEcl; ++k) ecl[k] = make_double2(INFINITY, -INFINITY);
 
-    auto star_ecl = [&](int by, double x, double y, double z) {  // grid.rs:49-73
-        const bool roche = by == 1 ? M.roche1 : M.roche2;
-        double a, b;
-        if (roche) {
-            if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, x, y, z, a, b, capped)) {
-                ing[necl] = a; eg[necl] = b; ++necl;
-            }
-        } else {
-            double l1, l2;
-            if (sphere_phase(M.cosi_e, M.sini_e, x, y, z, by == 1 ? 0.0 : 1.0, by == 1 ? M.r1 : M.r2, a, b, l1, l2)) {
-                ing[necl] = a; eg[necl] = b; ++necl;
-            }
-        }
+    // analytic eclipse by a spherical star (grid.rs:49-73); Roche stars go to k_roche
+    auto sphere_ecl = [&](int by, int slot) {
+        if (by == 1 ? M.roche1 : M.roche2) return;
+        double a, b, l1, l2;
+        if (sphere_phase(M.cosi_e, M.sini_e, px, py, pz, by == 1 ? 0.0 : 1.0, by == 1 ? M.r1 : M.r2, a, b, l1, l2))
+            ecl[slot] = make_double2(a, b);
+    };
+    auto disc_ecl = [&](double rdisc1, int slot) {
+        double a[2], b[2];
+        int n = disc_eclipse(M, rdisc1, px, py, pz, a, b);
+        for (int k = 0; k < n; ++k) ecl[slot + k] = make_double2(a[k], b[k]);
     };
 
-    if (valid) {
-        if (sg.kind == SEG_STAR1 || sg.kind == SEG_STAR2) {
-            const bool primary = sg.kind == SEG_STAR1;
-            // band of element i (grid.rs:227-262)
-            int lo = 0, hi = sg.ntable - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (A.bands[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
-            }
-            const Band b = A.bands[sg.table + lo];
-            const int64_t np = i - b.first;
-            double phi = b.phi1 + (b.phi2 - b.phi1) * ((double)np + 0.5) / (double)b.nphi;
-            double sinp, cosp;
-            sincos(phi, &sinp, &cosp);
-            double ux, uy, uz;
-            if (M.npole) { ux = b.sint * cosp; uy = b.sint * sinp; uz = b.cost; }
-            else { ux = b.cost; uy = b.sint * cosp; uz = b.sint * sinp; }
-            const bool roche = primary ? M.roche1 : M.roche2;
-            const double cofm = primary ? 0.0 : 1.0;
-            double rad, g;
-            if (roche) {  // face (surface.rs:54-121)
-                const double ssq = primary ? sq(M.spin1) : sq(M.spin2);
-                const double rref = primary ? M.rref1 : M.rref2, pref = primary ? M.pref1 : M.pref2;
-                double rlo = rref / 2.0, rhi = rref, t = pref + 1.0;
-                for (int k = 0; k < 30 && t > pref; ++k) {
-                    rlo = rhi / 2.0;
-                    t = pot_exact(primary, M.q, ssq, cofm + rlo * ux, rlo * uy, rlo * uz);
-                    if (t > pref) rhi = rlo;
-                }
-                for (int k = 0; k < 100 && rhi - rlo > M.acc_face; ++k) {
-                    double mid = (rlo + rhi) / 2.0;
-                    if (pot_exact(primary, M.q, ssq, cofm + mid * ux, mid * uy, mid * uz) < pref) rlo = mid;
-                    else rhi = mid;
-                }
-                rad = (rlo + rhi) / 2.0;
-                px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
-                double gx, gy, gz;
-                dpot_exact(primary, M.q, ssq, px, py, pz, gx, gy, gz);
-                g = sqrt(gx * gx + gy * gy + gz * gz);
-                double n2 = gx * gx + gy * gy + gz * gz;
-                if (n2 > 0.0) { double nn = sqrt(n2); dx = gx / nn; dy = gy / nn; dz = gz / nn; }
-                else { dx = gx; dy = gy; dz = gz; }
-            } else {
-                rad = primary ? M.r1 : M.r2;
-                px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
-                dx = ux; dy = uy; dz = uz;
-                g = 1.0;
-            }
-            area = (float)(((b.aphi * rad) * b.sint) * (b.ath * rad) / (ux * dx + uy * dy + uz * dz));
-            grav = (float)(g / (primary ? M.gref1 : M.gref2));
-            if (primary ? M.eclipse1 : M.eclipse2) star_ecl(primary ? 2 : 1, px, py, pz);
-            nse = necl;
-            if (M.add_disc && M.opaque)  // orchestration.rs:145-157
-                necl += disc_eclipse(M, M.rdisc1_l, px, py, pz, ing + necl, eg + necl);
-            // continuum (brightness.rs:49-144)
-            const double cx = primary ? 1.0 : 0.0;
-            double vx = cx - px, vy = -py, vz = -pz;
-            double r = sqrt(vx * vx + vy * vy + vz * vz);
-            double mu = (dx * vx + dy * vy + dz * vz) / r;
-            double geom, temp;
-            if (primary) {
-                double t1 = M.t1, plen = sqrt(px * px + py * py + pz * pz);
-                for (int k = 0; k < 3; ++k) {
-                    const SpotDev& s = M.spot1[k];
-                    if (!s.on) continue;
-                    double dist = ang_dist(px, py, pz, s, plen);
-                    t1 += (s.tcen - M.t1) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
-                }
-                if (M.uesp_on) {
-                    double el = sqrt(px * px + py * py);
-                    if (el > 0.0) {
-                        double clat = fmin(fmax((px * px + py * py) / el / plen, -1.0), 1.0);
-                        double dlat = rad2deg(acos(clat));
-                        double clong = fmin(fmax((M.uesp_dx * px + M.uesp_dy * py) / el, -1.0), 1.0);
-                        double dlong = rad2deg(acos(clong));
-                        double hw = M.uesp_lathw, lw = M.uesp_longhw, tp = M.uesp_taper, ut = M.uesp_temp;
-                        if (dlat <= hw && dlong <= lw) t1 = ut;
-                        else if (dlat <= hw) t1 += (ut - M.t1) * exp(-(dlong - lw) / tp);
-                        else if (dlong <= lw) t1 += (ut - M.t1) * exp(-(dlat - hw) / tp);
-                        else t1 += (ut - M.t1) * exp(-(dlat - hw) / tp) * exp(-(dlong - lw) / tp);
-                    }
-                }
-                temp = irradiate(t1, (double)grav, M.gdcbol1, M.absorb, M.t2, mu, r, M.r2c, geom);
-                flux = (float)((double)area * planck_d(M.wavelength, temp));
-                if (M.mirror) flux += (float)((double)area * geom * M.planck_t2abs);
-            } else {
-                double t2 = fabs(M.t2);
-                for (int k = 0; k < 2; ++k) {
-                    const SpotDev& s = M.spot2[k];
-                    if (!s.on) continue;
-                    double ox = px - 1.0, oy = py, oz = pz;
-                    double dist = ang_dist(ox, oy, oz, s, sqrt(ox * ox + oy * oy + oz * oz));
-                    t2 += (s.tcen - t2) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
-                }
-                temp = irradiate(t2, (double)grav, M.gdcbol2, M.absorb, M.t1, mu, r, M.r1c, geom);
-                flux = (float)((double)area * planck_d(M.wavelength, temp));
-                if (M.mirror) flux += (float)((double)area * geom * M.planck_t1);
-            }
-        } else if (sg.kind == SEG_DISC) {  // grid.rs:356-390, brightness.rs:204-212
-            int lo = 0, hi = sg.ntable - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (A.rings[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
-            }
-            const Ring g = A.rings[sg.table + lo];
-            double th = kTwoPi * (double)(i - g.first) / (double)g.ntheta;
-            double st, ct;
-            sincos(th, &st, &ct);
-            px = g.rad * ct; py = g.rad * st; pz = g.h;
-            dx = -ct * g.sinp; dy = -st * g.sinp; dz = g.cosp;
-            area = (float)g.area;
-            if (M.opaque) necl += disc_eclipse(M, M.rdisc1_g, px, py, pz, ing + necl, eg + necl);
-            if (M.eclipse1) star_ecl(1, px, py, pz);
-            if (M.eclipse2) star_ecl(2, px, py, pz);
-            double r = sqrt(px * px + py * py + pz * pz);
-            flux = (float)(M.disc_bright * pow(r / M.rdisc2, M.texp_disc) * (double)area);
-        } else if (sg.kind == SEG_EDGE) {  // grid.rs:411-478, brightness.rs:215-239
-            const int64_t col = i / M.edge_nout, row = i - col * M.edge_nout;
-            double th = kTwoPi * (double)col / (double)M.edge_ntheta;
-            double st, ct;
-            sincos(th, &st, &ct);
-            const double rv = M.edge_rad, h = M.edge_h;
-            if (row == 0) {
-                px = kEfac * rv * ct; py = kEfac * rv * st; pz = kEfac * h;
-                area = (float)(M.edge_area / 2.0);
-            } else {
-                pz = -h + 2.0 * h * (double)(row - 1) / (double)(M.edge_nout - 1);
-                px = kEfac * rv * ct; py = kEfac * rv * st;
-                area = (float)M.edge_area;
-            }
-            dx = ct; dy = st; dz = 0.0;
-            if (M.opaque) necl += disc_eclipse(M, M.rdisc1_g, px, py, pz, ing + necl, eg + necl);
-            if (M.eclipse1) star_ecl(1, px, py, pz);
-            if (M.eclipse2) star_ecl(2, px, py, pz);
-            double vx = 1.0 - px, vy = -py, vz = -pz;
-            double r = sqrt(vx * vx + vy * vy + vz * vz);
-            double mu = (dx * vx + dy * vy + dz * vz) / r;
-            double temp, r2 = M.r2e, t4 = sq(M.tedge) * sq(M.tedge), i4 = sq(M.t2abs) * sq(M.t2abs);
-            if (mu >= r2) {
-                double geom = sq(r2 / r) * mu;
-                temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
-            } else if (mu > -r2) {
-                double x0 = -mu / r2;
-                double geom = sq(r2 / r) * r2 * (sqrt(1.0 - x0 * x0) * (2.0 + x0 * x0) / 3.0 - x0 * (kPi / 2.0 - asin(x0))) / kPi;
-                temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
-            } else {
-                temp = M.tedge;
-            }
-            flux = (float)((double)area * planck_d(M.wavelength, temp));
-        } else {  // SEG_SPOT: grid.rs:520-550
-            const int64_t k = i >> 1;
-            const bool tilted = (i & 1) == 0;
-            double dist = M.sfac_spot * (double)k / (double)(M.nspot - 1);
-            double f = M.length_spot * (dist - M.bmax);
-            px = M.bspot[0] + f * M.bvec[0]; py = M.bspot[1] + f * M.bvec[1]; pz = M.bspot[2] + f * M.bvec[2];
-            if (M.eclipse1) star_ecl(1, px, py, pz);
-            if (M.eclipse2) star_ecl(2, px, py, pz);
-            double bright = M.bright_ref * pow(dist / M.bmax, M.expon_spot) *
-                            exp(M.expon_spot / M.epow_spot - pow(dist, M.epow_spot));
-            area = (float)M.area_spot;
-            if (tilted) { dx = M.tvec[0]; dy = M.tvec[1]; dz = M.tvec[2]; flux = (float)(bright * (1.0 - M.cfrac_spot) * M.area_spot); }
-            else { dx = 0.0; dy = 0.0; dz = 1.0; flux = (float)(bright * M.cfrac_spot * M.area_spot); }
+    if (sg.kind == SEG_STAR1 || sg.kind == SEG_STAR2) {
+        const bool primary = sg.kind == SEG_STAR1;
+        // band of element i (grid.rs:227-262)
+        int lo = 0, hi = sg.ntable - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (A.bands[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
         }
-        // outputs
-        A.el_rec[sg.first + i] = make_float4((float)dx, (float)dy, (float)dz, flux);
-        A.el_pos[sg.first + i] = make_float4((float)px, (float)py, (float)pz, 0.f);
-        double2* e = A.el_ecl + (sg.first + i) * kMaxEcl;
-        for (int k = 0; k < kMaxEcl; ++k)
-            e[k] = k < necl ? make_double2(ing[k], eg[k]) : make_double2(INFINITY, -INFINITY);
+        const Band b = A.bands[sg.table + lo];
+        const int64_t np = i - b.first;
+        double phi = b.phi1 + (b.phi2 - b.phi1) * ((double)np + 0.5) / (double)b.nphi;
+        double sinp, cosp;
+        sincos(phi, &sinp, &cosp);
+        double ux, uy, uz;
+        if (M.npole) { ux = b.sint * cosp; uy = b.sint * sinp; uz = b.cost; }
+        else { ux = b.cost; uy = b.sint * cosp; uz = b.sint * sinp; }
+        const bool roche = primary ? M.roche1 : M.roche2;
+        const double cofm = primary ? 0.0 : 1.0;
+        double rad, g;
+        if (roche) {  // face (surface.rs:54-121)
+            const double ssq = primary ? sq(M.spin1) : sq(M.spin2);
+            const double rref = primary ? M.rref1 : M.rref2, pref = primary ? M.pref1 : M.pref2;
+            double rlo = rref / 2.0, rhi = rref, t = pref + 1.0;
+            for (int k = 0; k < 30 && t > pref; ++k) {
+                rlo = rhi / 2.0;
+                t = pot_exact(primary, M.q, ssq, cofm + rlo * ux, rlo * uy, rlo * uz);
+                if (t > pref) rhi = rlo;
+            }
+            for (int k = 0; k < 100 && rhi - rlo > M.acc_face; ++k) {
+                double mid = (rlo + rhi) / 2.0;
+                if (pot_exact(primary, M.q, ssq, cofm + mid * ux, mid * uy, mid * uz) < pref) rlo = mid;
+                else rhi = mid;
+            }
+            rad = (rlo + rhi) / 2.0;
+            px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
+            double gx, gy, gz;
+            dpot_exact(primary, M.q, ssq, px, py, pz, gx, gy, gz);
+            double n2 = gx * gx + gy * gy + gz * gz;
+            g = sqrt(n2);
+            if (n2 > 0.0) { dx = gx / g; dy = gy / g; dz = gz / g; }
+            else { dx = gx; dy = gy; dz = gz; }
+        } else {
+            rad = primary ? M.r1 : M.r2;
+            px = cofm + rad * ux; py = rad * uy; pz = rad * uz;
+            dx = ux; dy = uy; dz = uz;
+            g = 1.0;
+        }
+        area = (float)(((b.aphi * rad) * b.sint) * (b.ath * rad) / (ux * dx + uy * dy + uz * dz));
+        grav = (float)(g / (primary ? M.gref1 : M.gref2));
+        if (primary ? M.eclipse1 : M.eclipse2) sphere_ecl(primary ? 2 : 1, 0);
+        if (M.add_disc && M.opaque) disc_ecl(M.rdisc1_l, 1);  // orchestration.rs:145-157
+        // continuum (brightness.rs:49-144)
+        const double cx = primary ? 1.0 : 0.0;
+        double vx = cx - px, vy = -py, vz = -pz;
+        double r = sqrt(vx * vx + vy * vy + vz * vz);
+        double mu = (dx * vx + dy * vy + dz * vz) / r;
+        double geom, temp;
+        if (primary) {
+            double t1 = M.t1, plen = sqrt(px * px + py * py + pz * pz);
+            for (int k = 0; k < 3; ++k) {
+                const SpotDev& s = M.spot1[k];
+                if (!s.on) continue;
+                double dist = ang_dist(px, py, pz, s, plen);
+                t1 += (s.tcen - M.t1) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
+            }
+            if (M.uesp_on) {
+                double el = sqrt(px * px + py * py);
+                if (el > 0.0) {
+                    double clat = fmin(fmax((px * px + py * py) / el / plen, -1.0), 1.0);
+                    double dlat = rad2deg(acos(clat));
+                    double clong = fmin(fmax((M.uesp_dx * px + M.uesp_dy * py) / el, -1.0), 1.0);
+                    double dlong = rad2deg(acos(clong));
+                    double hw = M.uesp_lathw, lw = M.uesp_longhw, tp = M.uesp_taper, ut = M.uesp_temp;
+                    if (dlat <= hw && dlong <= lw) t1 = ut;
+                    else if (dlat <= hw) t1 += (ut - M.t1) * exp(-(dlong - lw) / tp);
+                    else if (dlong <= lw) t1 += (ut - M.t1) * exp(-(dlat - hw) / tp);
+                    else t1 += (ut - M.t1) * exp(-(dlat - hw) / tp) * exp(-(dlong - lw) / tp);
+                }
+            }
+            temp = irradiate(t1, (double)grav, M.gdcbol1, M.absorb, M.t2, mu, r, M.r2c, geom);
+            flux = (float)((double)area * planck_d(M.wavelength, temp));
+            if (M.mirror) flux += (float)((double)area * geom * M.planck_t2abs);
+        } else {
+            double t2 = fabs(M.t2);
+            for (int k = 0; k < 2; ++k) {
+                const SpotDev& s = M.spot2[k];
+                if (!s.on) continue;
+                double ox = px - 1.0, oy = py, oz = pz;
+                double dist = ang_dist(ox, oy, oz, s, sqrt(ox * ox + oy * oy + oz * oz));
+                t2 += (s.tcen - t2) * exp(-sq(dist / (s.fwhm / kFwhmEfac)) / 2.0);
+            }
+            temp = irradiate(t2, (double)grav, M.gdcbol2, M.absorb, M.t1, mu, r, M.r1c, geom);
+            flux = (float)((double)area * planck_d(M.wavelength, temp));
+            if (M.mirror) flux += (float)((double)area * geom * M.planck_t1);
+        }
+    } else if (sg.kind == SEG_DISC) {  // grid.rs:356-390, brightness.rs:204-212
+        int lo = 0, hi = sg.ntable - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (A.rings[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
+        }
+        const Ring g = A.rings[sg.table + lo];
+        double th = kTwoPi * (double)(i - g.first) / (double)g.ntheta;
+        double st, ct;
+        sincos(th, &st, &ct);
+        px = g.rad * ct; py = g.rad * st; pz = g.h;
+        dx = -ct * g.sinp; dy = -st * g.sinp; dz = g.cosp;
+        area = (float)g.area;
+        if (M.opaque) disc_ecl(M.rdisc1_g, 0);
+        if (M.eclipse1) sphere_ecl(1, 2);
+        if (M.eclipse2) sphere_ecl(2, 3);
+        double r = sqrt(px * px + py * py + pz * pz);
+        flux = (float)(M.disc_bright * pow(r / M.rdisc2, M.texp_disc) * (double)area);
+    } else if (sg.kind == SEG_EDGE) {  // grid.rs:411-478, brightness.rs:215-239
+        const int64_t col = i / M.edge_nout, row = i - col * M.edge_nout;
+        double th = kTwoPi * (double)col / (double)M.edge_ntheta;
+        double st, ct;
+        sincos(th, &st, &ct);
+        const double rv = M.edge_rad, h = M.edge_h;
+        if (row == 0) {
+            px = kEfac * rv * ct; py = kEfac * rv * st; pz = kEfac * h;
+            area = (float)(M.edge_area / 2.0);
+        } else {
+            pz = -h + 2.0 * h * (double)(row - 1) / (double)(M.edge_nout - 1);
+            px = kEfac * rv * ct; py = kEfac * rv * st;
+            area = (float)M.edge_area;
+        }
+        dx = ct; dy = st; dz = 0.0;
+        if (M.opaque) disc_ecl(M.rdisc1_g, 0);
+        if (M.eclipse1) sphere_ecl(1, 2);
+        if (M.eclipse2) sphere_ecl(2, 3);
+        double vx = 1.0 - px, vy = -py, vz = -pz;
+        double r = sqrt(vx * vx + vy * vy + vz * vz);
+        double mu = (dx * vx + dy * vy + dz * vz) / r;
+        double temp, r2 = M.r2e, t4 = sq(M.tedge) * sq(M.tedge), i4 = sq(M.t2abs) * sq(M.t2abs);
+        if (mu >= r2) {
+            double geom = sq(r2 / r) * mu;
+            temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
+        } else if (mu > -r2) {
+            double x0 = -mu / r2;
+            double geom = sq(r2 / r) * r2 * (sqrt(1.0 - x0 * x0) * (2.0 + x0 * x0) / 3.0 - x0 * (kPi / 2.0 - asin(x0))) / kPi;
+            temp = pow(t4 + M.absorb_edge * i4 * geom, 0.25);
+        } else {
+            temp = M.tedge;
+        }
+        flux = (float)((double)area * planck_d(M.wavelength, temp));
+    } else {  // SEG_SPOT: grid.rs:520-550
+        const int64_t k = i >> 1;
+        const bool tilted = (i & 1) == 0;
+        double dist = M.sfac_spot * (double)k / (double)(M.nspot - 1);
+        double f = M.length_spot * (dist - M.bmax);
+        px = M.bspot[0] + f * M.bvec[0]; py = M.bspot[1] + f * M.bvec[1]; pz = M.bspot[2] + f * M.bvec[2];
+        if (M.eclipse1) sphere_ecl(1, 2);
+        if (M.eclipse2) sphere_ecl(2, 3);
+        double bright = M.bright_ref * pow(dist / M.bmax, M.expon_spot) *
+                        exp(M.expon_spot / M.epow_spot - pow(dist, M.epow_spot));
+        area = (float)M.area_spot;
+        if (tilted) { dx = M.tvec[0]; dy = M.tvec[1]; dz = M.tvec[2]; flux = (float)(bright * (1.0 - M.cfrac_spot) * M.area_spot); }
+        else { dx = 0.0; dy = 0.0; dz = 1.0; flux = (float)(bright * M.cfrac_spot * M.area_spot); }
+    }
+    const int64_t e = sg.first + i;
+    A.el_rec[e] = make_float4((float)dx, (float)dy, (float)dz, flux);
+    A.el_pos[e] = make_float4((float)px, (float)py, (float)pz, 0.f);
+    A.el_p64[e] = make_double4(px, py, pz, (double)area);
+    A.el_d64[e] = make_double4(dx, dy, dz, (double)grav);
+    double2* ep = A.el_ecl + e * kMaxEcl;
+    for (int k = 0; k < kMaxEcl; ++k) ep[k] = ecl[k];
+}
+
+// ---------------------------------------------------------------------------
+// k_roche: FP64 Roche ray-march of one element per thread (eclipse.rs:270-373)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs A) {
+    const ElemBlock blk = A.rblocks[blockIdx.x];
+    const SegDesc sg = A.segs[blk.seg];
+    const int64_t i = blk.offset + threadIdx.x;
+    EclCount cnt;
+    bool capped = false;
+    if (i < sg.count) {
+        const ModelDev& M = A.models[sg.model];
+        const int by = blk.by;
+        const int64_t e = sg.first + i;
+        const double4 p = A.el_p64[e];
+        double a, b;
+        if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt))
+            A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, by)] = make_double2(a, b);
         if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
     }
+    if (A.counters) {  // eclipse-search work counters, one atomic per warp and counter
+        unsigned long long v[5] = {(unsigned long long)cnt.pot, (unsigned long long)cnt.dpot,
+                                   (unsigned long long)cnt.fbl, (unsigned long long)cnt.cert,
+                                   (unsigned long long)cnt.skipped};
+        for (int k = 0; k < 5; ++k) {
+            unsigned long long x = v[k];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if ((threadIdx.x & 31) == 0 && x) atomicAdd(A.counters + k, x);
+        }
+    }
+}
 
-    // ---- per-model FP64 reductions (star segments only; block-uniform branch)
-    if (sg.kind != SEG_STAR1 && sg.kind != SEG_STAR2) return;
+// ---------------------------------------------------------------------------
+// k_aux: per-model FP64 sums over the star grids -- comp_star1/2 at the ginterp
+// and wdwarf phases (flux.rs:115-206), log g (flux.rs:288-322), radii (347-373)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kElemThreads) k_aux(ElemArgs A) {
+    const ElemBlock blk = A.ablocks[blockIdx.x];
+    const SegDesc sg = A.segs[blk.seg];
+    const ModelDev& M = A.models[sg.model];
+    const int64_t i = blk.offset + threadIdx.x;
+    const bool valid = i < sg.count;
     const int star = sg.kind == SEG_STAR1 ? 1 : 2;
+    double px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 0, area = 0, grav = 0, flux = 0;
+    double2 ecl[kMaxEcl];
+    if (valid) {
+        const int64_t e = sg.first + i;
+        double4 p = A.el_p64[e], d = A.el_d64[e];
+        px = p.x; py = p.y; pz = p.z; area = p.w;
+        dx = d.x; dy = d.y; dz = d.z; grav = d.w;
+        flux = (double)A.el_rec[e].w;
+        for (int k = 0; k < kMaxEcl; ++k) ecl[k] = A.el_ecl[e * kMaxEcl + k];
+    }
     double vals[16];
     int slot[16];
     int nv = 0;
@@ -639,11 +770,12 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
         bool match = sg.role == ROLE_BOTH || (sg.role == ROLE_FINE) == (sp.fine != 0);
         if (!match) continue;
         double c = 0.0;
-        if (valid) {  // comp_star1 / comp_star2 at one phase (flux.rs:115-206)
+        if (valid) {
+            // the ginterp sums run before the opaque-disc pairs exist (orchestration.rs:93-157)
+            const int ne = sp.star_ecl_only ? 1 : kMaxEcl;
             bool vis = true;
-            int ne = sp.star_ecl_only ? nse : necl;
             for (int k = 0; k < ne; ++k)
-                if ((sp.phi >= ing[k] && sp.phi <= eg[k]) || sp.phi <= eg[k] - 1.0) vis = false;
+                if ((sp.phi >= ecl[k].x && sp.phi <= ecl[k].y) || sp.phi <= ecl[k].y - 1.0) vis = false;
             double mu = sp.ex * dx + sp.ey * dy + sp.ez * dz;
             const double* ld = star == 1 ? M.ld1 : M.ld2;
             int lt = star == 1 ? M.ltype1 : M.ltype2;
@@ -654,9 +786,9 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
                     double vxx = -M.vfac * py, vyy = M.vfac * (px - M.xcofm);
                     double vr = -(sp.ex * vxx + sp.ey * vyy), vn = dx * vxx + dy * vyy;
                     double mud = mu - mu * vr - vn;
-                    c = mu * mag * (double)flux * (1.0 - beam * vr) * imu_d(ld, lt, mud);
+                    c = mu * mag * flux * (1.0 - beam * vr) * imu_d(ld, lt, mud);
                 } else {
-                    c = mu * mag * (double)flux * imu_d(ld, lt, mu);
+                    c = mu * mag * flux * imu_d(ld, lt, mu);
                 }
             }
         }
@@ -665,18 +797,16 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
         ++nv;
     }
     if (sg.fine_star) {
-        double fg = valid ? (double)flux * (double)grav : 0.0, ff = valid ? (double)flux : 0.0;
         double sa = 0.0, vol = 0.0;
         if (valid) {
-            double cx = star == 1 ? 0.0 : 1.0;
-            double wx = px - cx, wy = py, wz = pz;
+            double wx = px - (star == 1 ? 0.0 : 1.0), wy = py, wz = pz;
             double r = sqrt(wx * wx + wy * wy + wz * wz);
             double rc = dx * wx + dy * wy + dz * wz;
-            sa = (double)area * rc / ((r * r) * r);
-            vol = (double)area * rc;
+            sa = area * rc / ((r * r) * r);
+            vol = area * rc;
         }
-        vals[nv] = fg; slot[nv++] = star == 1 ? AUX_FG1 : AUX_FG2;
-        vals[nv] = ff; slot[nv++] = star == 1 ? AUX_F1 : AUX_F2;
+        vals[nv] = flux * grav; slot[nv++] = star == 1 ? AUX_FG1 : AUX_FG2;
+        vals[nv] = flux; slot[nv++] = star == 1 ? AUX_F1 : AUX_F2;
         vals[nv] = sa; slot[nv++] = star == 1 ? AUX_SA1 : AUX_SA2;
         vals[nv] = vol; slot[nv++] = star == 1 ? AUX_VOL1 : AUX_VOL2;
     }
@@ -690,9 +820,9 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
     }
     __syncthreads();
     if (threadIdx.x < nv) {
-        double s = 0.0;
-        for (int w = 0; w < kElemThreads / 32; ++w) s += red[threadIdx.x][w];
-        atomicAdd(A.aux + (int64_t)sg.model * kNumAux + slot[threadIdx.x], s);
+        double t = 0.0;
+        for (int w = 0; w < kElemThreads / 32; ++w) t += red[threadIdx.x][w];
+        atomicAdd(A.aux + (int64_t)sg.model * kNumAux + slot[threadIdx.x], t);
     }
 }
 
@@ -788,14 +918,21 @@ __device__ __forceinline__ int pair_cls(double ing, double eg, double lo, double
     return CLS_MIX;
 }
 
-__device__ __forceinline__ int classify(const double2* e, const double* rlo, const double* rhi) {
+// Moves the used pairs of one element to the front (empty pairs anywhere in
+// the slots) and classifies the element against the tile's phase range.
+__device__ __forceinline__ int classify(double2* e, const double* rlo, const double* rhi) {
+    int n = 0;
+    for (int k = 0; k < kMaxEcl; ++k) {
+        double2 p = e[k];
+        if (p.x <= 2.0) e[n++] = p;
+    }
+    for (int k = n; k < kMaxEcl; ++k) e[k] = make_double2(INFINITY, -INFINITY);
     int res = -1;
     for (int h = 0; h < 2; ++h) {
         if (!(rlo[h] <= rhi[h])) continue;  // empty half
         int c = CLS_VIS;
-        for (int k = 0; k < kMaxEcl; ++k) {
+        for (int k = 0; k < n; ++k) {
             double2 p = e[k];
-            if (!(p.x <= 2.0)) break;  // unused pair
             int pc = pair_cls(p.x, p.y, rlo[h], rhi[h]);
             if (pc == CLS_HID) { c = CLS_HID; break; }
             if (pc == CLS_MIX) c = CLS_MIX;
@@ -1190,7 +1327,52 @@ __global__ void __launch_bounds__(kEpiThreads) k_epilogue(EpiArgs A) {
     }
 }
 
+// FMA throughput microbenchmark: 8 independent FMA chains per thread.
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters, T seed) {
+    T a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = seed + (T)(threadIdx.x + k);
+    const T b = (T)0.999999, c = (T)1e-7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = a[k] * b + c;
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == (T)-12345.0) out[0] = s;  // keeps the chains live
+}
+
 }  // namespace
+
+cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflops) {
+    void* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, 16);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = num_sms * 8, threads = 256, iters = fp64 ? 4096 : 8192;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(a, s);
+        if (fp64) k_fma_peak<double><<<blocks, threads, 0, s>>>((double*)out, iters, 1.0);
+        else k_fma_peak<float><<<blocks, threads, 0, s>>>((float*)out, iters, 1.0f);
+        cudaEventRecord(b, s);
+        e = cudaEventSynchronize(b);
+        if (e != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    *tflops = best;
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
 
 size_t flux_smem_bytes() { return flux_smem_bytes_impl(); }
 
@@ -1218,10 +1400,27 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_elements(const ElemArgs& a, cudaStream_t s) {
-    if (a.nblocks <= 0) return cudaSuccess;
-    k_elements<<<(unsigned)a.nblocks, kElemThreads, 0, s>>>(a);
+    if (a.nblocks > 0) {
+        k_elements<<<(unsigned)a.nblocks, kElemThreads, 0, s>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_roche(const ElemArgs& a, cudaStream_t s) {
+    if (a.nrblocks <= 0) return cudaSuccess;
+    k_roche<<<(unsigned)a.nrblocks, kRocheBlock, 0, s>>>(a);
     return cudaGetLastError();
 }
+
+cudaError_t launch_aux(const ElemArgs& a, cudaStream_t s) {
+    if (a.nablocks <= 0) return cudaSuccess;
+    k_aux<<<(unsigned)a.nablocks, kElemThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+int roche_block_size() { return kRocheBlock; }
 
 cudaError_t launch_flux(const FluxArgs& a, int grid, cudaStream_t s) {
     if (a.nunits <= 0) return cudaSuccess;

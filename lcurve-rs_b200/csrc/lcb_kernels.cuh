@@ -11,15 +11,20 @@ namespace lcb {
 struct ElemArgs {
     const ModelDev* models;
     const SegDesc* segs;
-    const ElemBlock* blocks;
+    const ElemBlock* blocks;   // k_elements: every element
+    const ElemBlock* rblocks;  // k_roche: elements eclipsed by a Roche-distorted star (by = 1 or 2)
+    const ElemBlock* ablocks;  // k_aux: star-grid elements
     const Band* bands;
     const Ring* rings;
     float4* el_rec;      // dirn.xyz, flux
     float4* el_pos;      // posn.xyz, 0
+    double4* el_p64;     // posn.xyz, area (FP64)
+    double4* el_d64;     // dirn.xyz, gravity (FP64)
     double2* el_ecl;     // 4 (ingress, egress) pairs per element
     double* aux;         // kNumAux per model
     int* status;         // per model
-    int64_t nblocks;
+    int64_t nblocks, nrblocks, nablocks;
+    unsigned long long* counters;  // [pot evals, dpot evals, fblink calls, bound nodes, proven misses] or null
 };
 
 struct PhaseArgs {
@@ -69,8 +74,12 @@ struct EpiArgs {
 size_t flux_smem_bytes();
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s);
 cudaError_t launch_elements(const ElemArgs& a, cudaStream_t s);
+cudaError_t launch_roche(const ElemArgs& a, cudaStream_t s);
+cudaError_t launch_aux(const ElemArgs& a, cudaStream_t s);
+int roche_block_size();
 cudaError_t launch_flux(const FluxArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_epilogue(const EpiArgs& a, cudaStream_t s);
 int flux_blocks_per_sm();
+cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflops);
 
 }  // namespace lcb

@@ -676,17 +676,6 @@ void prepare_model(const Model& m, const lcb_datum* data, int64_t ndata, ModelLa
     }
 }
 
-// Rough cost of one element of the element kernel, in potential evaluations.
-int64_t element_cost(const ModelDev& D, const SegDesc& s) {
-    bool roche_ecl = false;
-    if (s.kind == SEG_STAR1) roche_ecl = D.eclipse1 && D.roche2;
-    else if (s.kind == SEG_STAR2) roche_ecl = D.eclipse2 && D.roche1;
-    else roche_ecl = (D.eclipse1 && D.roche1) || (D.eclipse2 && D.roche2);
-    int64_t c = 40;
-    if (roche_ecl) c += 4000;
-    return c;
-}
-
 }  // namespace
 
 double host_xl1(double q) { return l1_newton(q, -1.0 + q / (1.0 + q), 1.0 + 2.0 * (q / (1.0 + q)), -2.0 - q / (1.0 + q), 1.0, "xl1"); }
@@ -766,18 +755,25 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     }
     if (P.nelem > ((int64_t)1 << 34)) throw Error(LCB_ERR_INVALID, "batch too large (elements)");
 
-    // element-kernel blocks, heavy (Roche-eclipsed) segments first
-    std::vector<std::pair<int64_t, ElemBlock>> eb;
+    // element-kernel blocks; Roche ray-march blocks (one per eclipsing Roche star); star-grid aux blocks
     for (size_t s = 0; s < P.segs.size(); ++s) {
         const SegDesc& g = P.segs[s];
-        int64_t cost = element_cost(lay[g.model].dev, g);
-        if (cost > 1000) P.roche_elems += g.count;
-        for (int64_t off = 0; off < g.count; off += kElemThreads)
-            eb.push_back({cost, ElemBlock{(int32_t)s, 0, off}});
+        const ModelDev& D = lay[g.model].dev;
+        for (int64_t off = 0; off < g.count; off += kElemThreads) P.eblocks.push_back(ElemBlock{(int32_t)s, 0, off});
+        bool star = g.kind == SEG_STAR1 || g.kind == SEG_STAR2;
+        if (star)
+            for (int64_t off = 0; off < g.count; off += kElemThreads) P.ablocks.push_back(ElemBlock{(int32_t)s, 0, off});
+        for (int by = 1; by <= 2; ++by) {
+            bool roche = by == 1 ? D.roche1 : D.roche2;
+            bool ecl;
+            if (g.kind == SEG_STAR1) ecl = by == 2 && D.eclipse1;
+            else if (g.kind == SEG_STAR2) ecl = by == 1 && D.eclipse2;
+            else ecl = by == 1 ? D.eclipse1 : D.eclipse2;
+            if (!(roche && ecl)) continue;
+            P.roche_elems += g.count;
+            for (int64_t off = 0; off < g.count; off += kRocheBlock) P.rblocks.push_back(ElemBlock{(int32_t)s, by, off});
+        }
     }
-    std::stable_sort(eb.begin(), eb.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    P.eblocks.reserve(eb.size());
-    for (auto& x : eb) P.eblocks.push_back(x.second);
 
     // flux work units: choose the element range so there are a few units per resident block
     int64_t total = 0;
@@ -846,7 +842,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
 
     // shape key: what the device buffers and the captured graph depend on
     P.shape_key = {n, P.nelem, P.nsub, P.ndatum, P.npartial, (int64_t)P.units.size(), (int64_t)P.eblocks.size(),
-                   (int64_t)P.segs.size(), (int64_t)P.bands.size(), (int64_t)P.rings.size()};
+                   (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(), (int64_t)P.segs.size(),
+                   (int64_t)P.bands.size(), (int64_t)P.rings.size()};
 }
 
 }  // namespace lcb

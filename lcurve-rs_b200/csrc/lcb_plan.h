@@ -14,7 +14,9 @@ struct Plan {
     std::vector<SegDesc> segs;
     std::vector<Band> bands;
     std::vector<Ring> rings;
-    std::vector<ElemBlock> eblocks;
+    std::vector<ElemBlock> eblocks;    // k_elements
+    std::vector<ElemBlock> rblocks;    // k_roche
+    std::vector<ElemBlock> ablocks;    // k_aux
     std::vector<FluxUnit> units;
     std::vector<int32_t> datum_model;   // per (model, datum): model index
     std::vector<int64_t> datum_sub0;    // per (model, datum): first global sub-phase
