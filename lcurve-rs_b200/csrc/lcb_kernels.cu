@@ -39,8 +39,14 @@ constexpr double kFac2 = 1.0e9 * 6.6262e-34 * 2.99792458e8 / 1.3806e-23;  // pla
 constexpr double kFwhmEfac = 2.3548200450309493;                  // brightness.rs:8
 constexpr double kEfac = 1.0000001;                               // grid.rs:396
 constexpr int kFblinkEvalCap = 1 << 18;  // bound on one line-of-sight search (reference has none)
-constexpr int kRocheMinBlocks = 4;
-constexpr int kCertBudget = 32;   // lower-bound nodes per line of sight before the full search
+#ifndef LCB_ROCHE_MIN_BLOCKS
+#define LCB_ROCHE_MIN_BLOCKS 4
+#endif
+#ifndef LCB_CERT_BUDGET
+#define LCB_CERT_BUDGET 32
+#endif
+constexpr int kRocheMinBlocks = LCB_ROCHE_MIN_BLOCKS;  // k_roche blocks per SM (128 threads): register budget
+constexpr int kCertBudget = LCB_CERT_BUDGET;           // lower-bound nodes per line of sight before the full search
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 __device__ __forceinline__ double rad2deg(double r) { return r * (180.0 / kPi); }
@@ -322,39 +328,54 @@ __device__ bool sphere_phase(double cosi, double sini, double px, double py, dou
 }
 
 // Ingress/egress of point p behind a Roche-distorted star (eclipse.rs:270-373).
+// The phase scan of pot_min_search (eclipse.rs:347-373) and the two bisections
+// (eclipse.rs:301-332) run as one loop with a single line-of-sight search call
+// site: lanes of a warp in different stages reconverge inside the search, and
+// the search code exists once.  Misses are proven (fblink's `prove`) only in the
+// scan, where nearly all lines of sight miss by a wide margin.
 __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
                                double pz, double& ing, double& eg, bool& capped, EclCount& evals) {
     double phi1, phi2, lam1, lam2;
     if (!sphere_phase(cosi, sini, px, py, pz, s.cofmx, s.rref, phi1, phi2, lam1, lam2)) return false;
     double acc = 2.0 * sqrt(2.0 * kTwoPi * (lam2 - lam1) * delta);
     Los L{px, py, pz, 0.0, 0.0, 0.0};
-    // pot_min_search: first scanned phase that is eclipsed (eclipse.rs:347-373)
     double ns = ceil((phi2 - phi1) / (acc / kTwoPi));
-    int nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
-    double dphi = (phi2 - phi1) / (double)nsteps;
-    double phi = 0.0;
-    bool found = false;
-    for (int i = 0; i <= nsteps; ++i) {
-        phi = phi1 + (double)i * dphi;
-        earth_at(cosi, sini, phi, L.ex, L.ey, L.ez);
-        if (fblink(s, acc, L, evals, capped, true)) { found = true; break; }
-        if (capped) return false;
-    }
-    if (!found) return false;
-    auto chop = [&](double pin, double pout) {
-        for (int it = 0; it < 200 && fabs(pin - pout) > delta; ++it) {
-            double pmid = (pin + pout) / 2.0;
-            earth_at(cosi, sini, pmid, L.ex, L.ey, L.ez);
-            if (fblink(s, acc, L, evals, capped, false)) pin = pmid; else pout = pmid;
+    const int nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
+    const double dphi = (phi2 - phi1) / (double)nsteps;
+    enum { SCAN, CHOP_IN, CHOP_EG };
+    int mode = SCAN, i = 0, it = 0;
+    double phi = 0.0, pin = 0.0, pout = 0.0;
+    for (;;) {
+        double ph;
+        if (mode == SCAN) {
+            if (i > nsteps) return false;  // no eclipsed phase found
+            ph = phi1 + (double)i * dphi;
+        } else {
+            if (!(fabs(pin - pout) > delta) || it >= 200) {
+                double r = (pin + pout) / 2.0;
+                r -= floor(r);
+                if (mode == CHOP_IN) {
+                    ing = r;
+                    mode = CHOP_EG; pin = phi; pout = phi2; it = 0;
+                    continue;
+                }
+                eg = r;
+                if (eg < ing) eg += 1.0;
+                return true;
+            }
+            ph = (pin + pout) / 2.0;
         }
-        return (pin + pout) / 2.0;
-    };
-    ing = chop(phi, phi1);
-    ing -= floor(ing);
-    eg = chop(phi, phi2);
-    eg -= floor(eg);
-    if (eg < ing) eg += 1.0;
-    return true;
+        earth_at(cosi, sini, ph, L.ex, L.ey, L.ez);
+        const bool hit = fblink(s, acc, L, evals, capped, mode == SCAN && kCertBudget > 0);
+        if (capped) return false;
+        if (mode == SCAN) {
+            if (hit) { phi = ph; mode = CHOP_IN; pin = phi; pout = phi1; it = 0; }
+            else ++i;
+        } else {
+            if (hit) pin = ph; else pout = ph;
+            ++it;
+        }
+    }
 }
 
 // Disc occultation (disc_eclipse.rs:29-70, 84-330); returns the number of pairs (<= 2).
@@ -902,7 +923,6 @@ enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
 
 struct FluxSmem {
     float4 rec[2][kFluxChunk];
-    float4 pos[2][kFluxChunk];
     double2 ecl[2][kFluxChunk * kMaxEcl];
     int8_t cls[kFluxChunk];
     uint64_t bar[2];
@@ -942,6 +962,28 @@ __device__ __forceinline__ int classify(double2* e, const double* rlo, const dou
     }
     return res < 0 ? CLS_HID : res;
 }
+
+// The earth vector of phase theta/2pi is (sini cos t, -sini sin t, cosi), so an
+// element's mu over a phase arc is A cos t + B sin t + C.  The tile's active
+// sub-phases lie on (at most) two arcs shorter than pi, one per half of [0, 1).
+struct Arcs {
+    float ca[2], sa[2], cb[2], sb[2];
+    bool on[2];
+};
+// Largest mu of direction (dx, dy, dz) over the arcs (FP32; the caller keeps a margin).
+__device__ __forceinline__ float max_mu(const Arcs& a, float si, float ci, float dx, float dy, float dz) {
+    const float A = si * dx, B = -si * dy, C = ci * dz;
+    float m = -2.f;
+    for (int h = 0; h < 2; ++h) {
+        if (!a.on[h]) continue;
+        float in1 = a.ca[h] * B - a.sa[h] * A, in2 = A * a.sb[h] - B * a.cb[h];
+        float v = (in1 >= 0.f && in2 >= 0.f) ? sqrtf(A * A + B * B)
+                                              : fmaxf(A * a.ca[h] + B * a.sa[h], A * a.cb[h] + B * a.sb[h]);
+        m = fmaxf(m, v + C);
+    }
+    return m;
+}
+constexpr float kFacingMargin = 2e-5f;  // far above the FP32 rounding of mu
 
 __device__ __forceinline__ bool hidden_at(const double2* e, double phi) {
     bool h = false;
@@ -1049,6 +1091,14 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
     for (int w = 0; w < kFluxThreads / 32; ++w)
         for (int h = 0; h < 2; ++h) { rlo[h] = fmin(rlo[h], s_lo[w][h]); rhi[h] = fmax(rhi[h], s_hi[w][h]); }
     const bool any = rlo[0] <= rhi[0] || rlo[1] <= rhi[1];
+    Arcs arcs;
+    for (int h = 0; h < 2; ++h) {
+        arcs.on[h] = rlo[h] <= rhi[h];
+        float lo = arcs.on[h] ? (float)rlo[h] : 0.f, hi = arcs.on[h] ? (float)rhi[h] : 0.f;
+        sincospif(2.f * lo, &arcs.sa[h], &arcs.ca[h]);
+        sincospif(2.f * hi, &arcs.sb[h], &arcs.cb[h]);
+    }
+    const float sif = (float)M.sini_l, cif = (float)M.cosi_l;
 
     float acc_hi[kFluxR], acc_lo[kFluxR];
 #pragma unroll
@@ -1056,7 +1106,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 
     Contrib<KIND> C;
     C.setup(M, U.star);
-    const bool need_pos = KIND == UK_STAR_GENERIC;
+    const float face_thr = (KIND == UK_STAR_GENERIC ? (U.star == 1 ? M.mucrit1f : M.mucrit2f) : C.thr) - kFacingMargin;
     // generic-path constants
     const float* ldg = U.star == 1 ? M.ld1f : M.ld2f;
     const int ltg = U.star == 1 ? M.ltype1 : M.ltype2;
@@ -1070,12 +1120,11 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         int b = c & 1;
         int64_t e0 = U.e0 + (int64_t)c * kFluxChunk;
         int n = min(kFluxChunk, U.ne - c * kFluxChunk);
-        uint32_t bytes = (uint32_t)n * (16u + 16u * kMaxEcl + (need_pos ? 16u : 0u));
+        uint32_t bytes = (uint32_t)n * (16u + 16u * kMaxEcl);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect(&S.bar[b], bytes);
         bulk_load(S.rec[b], A.el_rec + e0, (uint32_t)n * 16u, &S.bar[b]);
         bulk_load(S.ecl[b], A.el_ecl + e0 * kMaxEcl, (uint32_t)n * 16u * kMaxEcl, &S.bar[b]);
-        if (need_pos) bulk_load(S.pos[b], A.el_pos + e0, (uint32_t)n * 16u, &S.bar[b]);
     };
     if (tid == 0) {
         if (nchunks > 0) issue(0);
@@ -1086,7 +1135,14 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         const int n = min(kFluxChunk, U.ne - c * kFluxChunk);
         if (!mbar_wait(&S.bar[b], parity[b])) atomicOr(A.status + U.model, kStatusTmaTimeout);
         parity[b] ^= 1u;
-        for (int e = tid; e < n; e += kFluxThreads) S.cls[e] = (int8_t)classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
+        for (int e = tid; e < n; e += kFluxThreads) {
+            int cl = classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
+            if (cl != CLS_HID) {  // never facing the observer on this tile: contributes exactly 0
+                const float4 r = S.rec[b][e];
+                if (max_mu(arcs, sif, cif, r.x, r.y, r.z) <= face_thr) cl = CLS_HID;
+            }
+            S.cls[e] = (int8_t)cl;
+        }
         __syncthreads();
         for (int s0 = 0; s0 < n; s0 += 32) {
             float part[kFluxR];
@@ -1098,7 +1154,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                 if (cls == CLS_HID) continue;
                 const float4 r = S.rec[b][e];
                 if (KIND == UK_STAR_GENERIC) {
-                    const float4 p = S.pos[b][e];
+                    const float4 p = __ldg(A.el_pos + U.e0 + (int64_t)c * kFluxChunk + e);
                     float vx, vy;
                     if (U.star == 1) { vx = -M.vfacf * spin * p.y; vy = M.vfacf * (spin * p.x - M.xcofmf); }
                     else { vx = -M.vfacf * spin * p.y; vy = M.vfacf * (spin * (p.x - 1.f) + 1.f - M.xcofmf); }
@@ -1164,7 +1220,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
     }
 }
 
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux(FluxArgs A) {
+__global__ void __launch_bounds__(kFluxThreads, 5) k_flux(FluxArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FluxSmem& S = *reinterpret_cast<FluxSmem*>(smem_raw);
     if (threadIdx.x == 0) {
