@@ -119,6 +119,26 @@ void lcb_free_data(lcb_datum* data);
 int lcb_light_curve(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
                     int scale, int rdata, double* calc_out, lcb_result* res_out);
 
+/* ---- light curve without device allocation ----------------------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc (device memory already claimed by another framework's pool
+ * allocator, plugin hosts that forbid allocation inside callbacks, loops that
+ * cannot afford the synchronisation cudaMalloc/cudaFree may imply).
+ * Same arguments, results and errors as lcb_light_curve, but every device
+ * buffer lives in one fixed arena of LCB_NOALLOC_ARENA_BYTES, a file-scope
+ * device array that each device loading this library holds until the process
+ * exits.  Nothing is allocated on the device: a model and data set needing
+ * more scratch than the arena is rejected with LCB_ERR_INVALID and a message
+ * giving the bytes needed (a grid element takes about 160 B, a datum about
+ * 80 B, each exposure sub-division about 40 B plus 8 B per 4,096 elements).
+ * The first call on a device looks up the arena's device address; make that
+ * first call before any CUDA stream capture begins.  All calls on a device share the arena: this library serialises
+ * them and waits for each call's GPU work before returning, since calls whose
+ * GPU work overlapped would race. */
+#define LCB_NOALLOC_ARENA_BYTES (64u * 1024u * 1024u)
+int lcb_light_curve_noalloc(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
+                            int scale, int rdata, double* calc_out, lcb_result* res_out);
+
 /* ---- grid inspection --------------------------------------------------------
  * The elements the GPU builds for one model -- the grids of set_star_grid /
  * set_disc_grid / set_disc_edge / set_bright_spot_grid after continuum and

@@ -45,6 +45,7 @@ SYMBOLS = [
     "lcb_light_curve", "lcb_chisq_batch", "lcb_chisq_batch_ragged", "lcb_batch_create", "lcb_batch_destroy",
     "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_profile", "lcb_batch_stage_ms",
     "lcb_ctx_transfer_bytes", "lcb_measure_fma_peak", "lcb_model_grid", "lcb_batch_search_counts",
+    "lcb_light_curve_noalloc",
 ]
 
 _lib = None
@@ -88,6 +89,7 @@ def load():
         "lcb_model_grid": ([vp, vp, i, i64p, dp, dp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                             C.POINTER(C.c_float), dp], i),
         "lcb_batch_search_counts": ([vp, i64p], i),
+        "lcb_light_curve_noalloc": ([vp, vp, vp, i64, i, i, dp, C.POINTER(Result)], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -732,3 +732,157 @@ int lcb_measure_fma_peak(lcb_ctx* C, int which, double* tflops) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// lcb_light_curve_noalloc: the light curve of one model with no device
+// allocation.
+//
+// Some callers cannot call cudaMalloc: a process whose device memory is
+// already claimed by another framework's pool allocator (JAX preallocating
+// most of the GPU, a serving runtime with a fixed memory budget), a plugin
+// host that forbids allocation inside its callbacks, or a timing-sensitive
+// loop that cannot afford the device-wide synchronisation cudaMalloc and
+// cudaFree may imply.  For them this entry point runs the same kernels as
+// lcb_light_curve, but every device buffer (plan tables, element and
+// sub-phase arrays, flux partials, results) is carved out of one statically
+// allocated arena of LCB_NOALLOC_ARENA_BYTES.  Host staging uses ordinary
+// pageable host memory.
+//
+// The arena is file-scope device memory: every device on which this
+// library's device code is loaded holds it until the process exits.  In host
+// code its name is only a host-side shadow; the device address is looked up
+// once per device (cudaGetSymbolAddress, with that device current) by the
+// first call on that device.
+//
+// Every call on a device shares the arena, which keeps the previous call's
+// contents.  The accumulators that must start at zero (per-model sums, status
+// words, the work-unit counter and search counters) are cleared by the launch
+// sequence itself; every other region is written in full before it is read.
+// Two calls whose GPU work overlapped would race on the arena, so calls on one
+// device are serialised by a per-device lock, and each call waits for its GPU
+// work (also on its error paths) before it returns.
+// ===========================================================================
+static __device__ __align__(256) unsigned char g_noalloc_arena[LCB_NOALLOC_ARENA_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu[kNoallocMaxDevices];   // one per device
+void* g_noalloc_base[kNoallocMaxDevices] = {};  // device address of the arena, per device
+
+// The arena's device address on the current device (set up on first use).
+// Caller holds g_noalloc_mu[device] and has made `device` current.
+unsigned char* noalloc_arena(int device) {
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
+        if (e != cudaSuccess || !p)
+            throw Error(LCB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc arena): ") + cudaGetErrorString(e));
+        g_noalloc_base[device] = p;
+    }
+    return static_cast<unsigned char*>(g_noalloc_base[device]);
+}
+
+// Lays out every buffer of a planned single-model evaluation inside the arena
+// (base == nullptr only measures).  Returns the bytes used.
+size_t noalloc_carve(const lcb::Plan& P, unsigned char* base, DeviceSet& D) {
+    size_t off = 0;
+    auto take = [&](DevBuf& b, size_t bytes) {
+        b.p = base ? base + off : nullptr;
+        b.cap = bytes;
+        off += (bytes + 255) & ~size_t(255);
+    };
+    const size_t nm = P.models.size();
+    take(D.models, nm * sizeof(lcb::ModelDev));
+    take(D.segs, P.segs.size() * sizeof(lcb::SegDesc));
+    take(D.bands, P.bands.size() * sizeof(lcb::Band));
+    take(D.rings, P.rings.size() * sizeof(lcb::Ring));
+    take(D.eblocks, P.eblocks.size() * sizeof(lcb::ElemBlock));
+    take(D.rblocks, P.rblocks.size() * sizeof(lcb::ElemBlock));
+    take(D.ablocks, P.ablocks.size() * sizeof(lcb::ElemBlock));
+    take(D.units, P.units.size() * sizeof(lcb::FluxUnit));
+    take(D.dmodel, P.datum_model.size() * sizeof(int32_t));
+    take(D.dsub0, P.datum_sub0.size() * sizeof(int64_t));
+    take(D.datum, P.ndatum * sizeof(lcb_datum));
+    take(D.rec, P.nelem * sizeof(float4));
+    take(D.pos, P.nelem * sizeof(float4));
+    take(D.p64, P.nelem * sizeof(double4));
+    take(D.d64, P.nelem * sizeof(double4));
+    take(D.ecl, P.nelem * lcb::kMaxEcl * sizeof(double2));
+    take(D.aux, nm * lcb::kNumAux * sizeof(double));
+    take(D.status, nm * sizeof(int));
+    take(D.spe, P.nsub * sizeof(float4));
+    take(D.spphi, P.nsub * sizeof(double));
+    take(D.sptype, P.nsub * sizeof(int8_t));
+    take(D.spw, P.nsub * sizeof(double));
+    take(D.slfac, P.ndatum * sizeof(double));
+    take(D.partial, P.npartial * sizeof(double));
+    take(D.calc, P.ndatum * sizeof(double));
+    take(D.results, nm * 12 * sizeof(double));
+    take(D.counter, sizeof(int) * 4);
+    take(D.ecount, sizeof(unsigned long long) * 8);
+    return off;
+}
+
+// Host -> arena copies of the plan's tables and the data (no allocation).
+void noalloc_upload(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* data) {
+    auto put = [&](DevBuf& b, const void* src, size_t bytes) {
+        if (bytes) CUDA_TRY(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, C->stream));
+        C->h2d += (int64_t)bytes;
+    };
+    put(D.models, P.models.data(), P.models.size() * sizeof(lcb::ModelDev));
+    put(D.segs, P.segs.data(), P.segs.size() * sizeof(lcb::SegDesc));
+    put(D.bands, P.bands.data(), P.bands.size() * sizeof(lcb::Band));
+    put(D.rings, P.rings.data(), P.rings.size() * sizeof(lcb::Ring));
+    put(D.eblocks, P.eblocks.data(), P.eblocks.size() * sizeof(lcb::ElemBlock));
+    put(D.rblocks, P.rblocks.data(), P.rblocks.size() * sizeof(lcb::ElemBlock));
+    put(D.ablocks, P.ablocks.data(), P.ablocks.size() * sizeof(lcb::ElemBlock));
+    put(D.units, P.units.data(), P.units.size() * sizeof(lcb::FluxUnit));
+    put(D.dmodel, P.datum_model.data(), P.datum_model.size() * sizeof(int32_t));
+    put(D.dsub0, P.datum_sub0.data(), P.datum_sub0.size() * sizeof(int64_t));
+    std::vector<lcb_datum> ex(P.ndatum);
+    for (int64_t d = 0; d < P.ndatum; ++d) ex[d] = data[P.datum_src[d]];
+    put(D.datum, ex.data(), ex.size() * sizeof(lcb_datum));
+}
+
+}  // namespace
+
+extern "C" int lcb_light_curve_noalloc(lcb_ctx* C, const lcb_model* model, const lcb_datum* data, int64_t n,
+                                       int scale, int rdata, double* calc_out, lcb_result* res_out) {
+    if (!C || !model || (!data && n > 0) || !calc_out) return fail(LCB_ERR_INVALID, "null pointer");
+    if (n <= 0) return fail(LCB_ERR_EMPTY, "No data points");
+    if (C->device < 0 || C->device >= kNoallocMaxDevices)
+        return fail(LCB_ERR_INVALID, "lcb_light_curve_noalloc: device index beyond the supported 64");
+    return guarded(C, [&] {
+        check_iscale(model->m);
+        const lcb::Model* mp = &model->m;
+        int64_t st = 0, cnt = n;
+        lcb::Plan P;
+        lcb::plan_batch(&mp, 1, data, &st, &cnt, C->num_sms, P);
+        if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
+        DeviceSet D;  // views into the arena: never ensure()d or released
+        const size_t need = noalloc_carve(P, nullptr, D);
+        if (need > (size_t)LCB_NOALLOC_ARENA_BYTES)
+            throw Error(LCB_ERR_INVALID, "lcb_light_curve_noalloc: this model and data need " + std::to_string(need) +
+                                             " bytes of device scratch, more than the fixed arena's " +
+                                             std::to_string((size_t)LCB_NOALLOC_ARENA_BYTES) +
+                                             "; use lcb_light_curve (or coarser grids / fewer points)");
+        std::lock_guard<std::mutex> lock(g_noalloc_mu[C->device]);
+        noalloc_carve(P, noalloc_arena(C->device), D);
+        std::vector<double> res, calc;
+        std::vector<int> status;
+        try {
+            noalloc_upload(C, D, P, data);
+            enqueue_run(C, D, P, scale, rdata, false);
+            fetch_results(C, D, P, res, &calc, &status);  // ends with a stream synchronise
+        } catch (...) {
+            cudaStreamSynchronize(C->stream);  // no work may touch the arena after the lock is released
+            throw;
+        }
+        if (status[0] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+        if (status[0] & lcb::kStatusIterCap)
+            throw Error(LCB_ERR_DEVICE_CHECK, "a device-side iteration cap tripped for this model");
+        std::memcpy(calc_out, calc.data(), n * sizeof(double));
+        if (res_out) fill_result(res.data(), res_out);
+    });
+}
