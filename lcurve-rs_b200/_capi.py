@@ -46,6 +46,10 @@ SYMBOLS = [
     "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_profile", "lcb_batch_stage_ms",
     "lcb_ctx_transfer_bytes", "lcb_measure_fma_peak", "lcb_model_grid", "lcb_batch_search_counts",
     "lcb_light_curve_noalloc",
+    # surrogate (lcurve_b200_surrogate.h)
+    "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
+    "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
+    "lcb_mlp_train_step", "lcb_mlp_take_loss", "lcb_mlp_sync", "lcb_mlp_gemm", "lcb_logflux_chisq",
 ]
 
 _lib = None
@@ -90,6 +94,21 @@ def load():
                             C.POINTER(C.c_float), dp], i),
         "lcb_batch_search_counts": ([vp, i64p], i),
         "lcb_light_curve_noalloc": ([vp, vp, vp, i64, i, i, dp, C.POINTER(Result)], i),
+        "lcb_mlp_last_error": ([], cp),
+        "lcb_mlp_create": ([i, i, i, i, i, i64, C.c_uint64, C.POINTER(vp)], i),
+        "lcb_mlp_destroy": ([vp], None),
+        "lcb_mlp_set_stream": ([vp, vp], i),
+        "lcb_mlp_num_params": ([vp, i64p], i),
+        "lcb_mlp_get_params": ([vp, vp, i64], i),
+        "lcb_mlp_set_params": ([vp, vp, i64], i),
+        "lcb_mlp_get_grads": ([vp, vp, i64], i),
+        "lcb_mlp_forward": ([vp, vp, i64, vp], i),
+        "lcb_mlp_backward": ([vp, vp, vp, i64], i),
+        "lcb_mlp_train_step": ([vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float], i),
+        "lcb_mlp_take_loss": ([vp, dp], i),
+        "lcb_mlp_sync": ([vp], i),
+        "lcb_mlp_gemm": ([i, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, vp], i),
+        "lcb_logflux_chisq": ([i64, i, vp, vp, vp, vp, vp, i, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -102,6 +121,13 @@ def load():
 def check(rc: int) -> None:
     if rc != LCB_OK:
         msg = load().lcb_last_error()
+        raise LcbError(rc, msg.decode() if msg else "")
+
+
+def check_mlp(rc: int) -> None:
+    """Status check for the surrogate entry points (their own error slot)."""
+    if rc != LCB_OK:
+        msg = load().lcb_mlp_last_error()
         raise LcbError(rc, msg.decode() if msg else "")
 
 

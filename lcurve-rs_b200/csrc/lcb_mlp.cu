@@ -1,0 +1,863 @@
+// lcb_mlp.cu — the light-curve surrogate: a small MLP trained and evaluated
+// with hand-written sm_100a BF16 tensor-core kernels.
+//
+// The network maps the five physical parameters of a binary (q, iangle, r1,
+// t1, t2, normalised by the caller) to a light curve on a fixed phase grid
+// (standardised log fluxes): n_in -> width x n_hidden (GELU) -> n_out.  It is
+// the cheap first stage of delayed-acceptance MCMC; the light-curve engine
+// stays the second-stage judge.
+//
+// GEMM kernel (k_gemm): C[M x N] = A[M x K] . B[N x K]^T, both operands BF16
+// row-major (K contiguous), FP32 accumulation in tensor memory:
+//   - one CTA per 128 x 128 output tile, four warps;
+//   - warp 0 lane 0 streams 128 x 64 K-slices of A and B into shared memory
+//     with TMA (cp.async.bulk.tensor, 128-byte swizzle), four stages on
+//     mbarriers;
+//   - warp 1 lane 0 issues tcgen05.mma (kind::f16, M=128, N=128, K=16) from
+//     shared-memory descriptors into a 128-column TMEM accumulator, and
+//     releases each stage with tcgen05.commit;
+//   - all four warps read the accumulator back with tcgen05.ld (warp w owns
+//     TMEM lanes 32w..32w+31 = tile rows) and apply the fused epilogue:
+//       EPI_F32        out = acc                                  (weight gradients)
+//       EPI_BIAS_GELU  z = acc + bias; out = bf16(gelu(z)); out2 = z  (hidden layers)
+//       EPI_BIAS_F32   out = acc + bias                           (output layer)
+//       EPI_DGELU      out = bf16(acc * gelu'(aux))               (backward through GELU)
+// Every mbarrier wait is bounded; a time-out sets the error word and the CTA
+// still releases its tensor memory.
+//
+// Training runs forward, backward (weight gradients as dZ^T . X with both
+// operands transposed into K-major copies, input gradients as dZ . W^T with a
+// transposed weight copy kept by the optimiser) and Adam on FP32 master
+// weights; every step is a fixed launch sequence on the network's stream.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/lcurve_b200.h"
+#include "../../include/lcurve_b200_surrogate.h"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4, GEMM_THREADS = 128;
+constexpr uint32_t TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
+
+enum { EPI_F32 = 0, EPI_BIAS_GELU = 1, EPI_BIAS_F32 = 2, EPI_DGELU = 3 };
+
+struct GemmSmem {
+    uint8_t a[STAGES][TILE_A];  // 1024-byte aligned slices (128-byte swizzle atoms)
+    uint8_t b[STAGES][TILE_B];
+    uint64_t full[STAGES], empty[STAGES], done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+struct GemmArgs {
+    int M, N, K;
+    const float* bias;
+    const float* aux;
+    void* out;
+    void* out2;
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t s_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t* b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_u32(b)));
+}
+__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(s_u32(b)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Bounded wait (about 2 s of SM clock).
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
+    if (bar_test(b, parity)) return true;
+    long long t0 = clock64();
+    while (!bar_test(b, parity)) {
+        __nanosleep(32);
+        if (clock64() - t0 > 4000000000LL) return false;
+    }
+    return true;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            s_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(s_u32(b))
+        : "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), descriptor version 1, base offset 0.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+    d |= (uint64_t)1 << 46;             // version
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
+}
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_u32(b)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+#define LCB_R8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : LCB_R8(0), LCB_R8(8), LCB_R8(16), LCB_R8(24)
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+#undef LCB_R8
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float dgelu(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// ---------------------------------------------------------------------------
+// k_gemm
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    k_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = s_u32(smem_raw);
+    GemmSmem& S = *reinterpret_cast<GemmSmem*>(smem_raw + (((raw + 1023u) & ~1023u) - raw));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int nk = (g.K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            bar_init(&S.full[s]);
+            bar_init(&S.empty[s]);
+        }
+        bar_init(&S.done);
+        S.abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&S.tmem_base)),
+                     "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem_base;
+
+    int issued = 0;  // TMA stages issued by the producer
+    if (warp == 0 && lane == 0) {
+        for (int kc = 0; kc < nk; ++kc) {
+            const int s = kc % STAGES;
+            if (kc >= STAGES && !bar_wait(&S.empty[s], ((kc / STAGES) - 1) & 1)) {
+                S.abort = 1;
+                break;
+            }
+            bar_expect(&S.full[s], TILE_A + TILE_B);
+            tma_load_2d(S.a[s], &ta, kc * BK, m0, &S.full[s]);
+            tma_load_2d(S.b[s], &tb, kc * BK, n0, &S.full[s]);
+            issued = kc + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        for (int kc = 0; kc < nk; ++kc) {
+            const int s = kc % STAGES;
+            if (!bar_wait(&S.full[s], (kc / STAGES) & 1)) {
+                S.abort = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint64_t da = sw128_desc(s_u32(S.a[s])), db = sw128_desc(s_u32(S.b[s]));
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) umma(tmem, da + 2 * kk, db + 2 * kk, (kc | kk) != 0);
+            umma_commit(&S.empty[s]);
+        }
+        umma_commit(&S.done);  // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+
+    const bool ok = __all_sync(0xffffffffu, bar_wait(&S.done, 0));
+    tc_fence_after();
+    const int r = m0 + warp * 32 + lane;
+    if (ok) {
+        for (int c0 = 0; c0 < BN && n0 + c0 < g.N; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (r < g.M) {
+                const int nb = n0 + c0;
+                const int nv = min(32, g.N - nb);  // multiple of 8 (N % 8 == 0)
+                const size_t row = (size_t)r * g.N + nb;
+                if (MODE == EPI_F32 || MODE == EPI_BIAS_F32) {
+                    float* o = reinterpret_cast<float*>(g.out) + row;
+                    for (int j = 0; j < nv; j += 4) {
+                        float4 q;
+                        q.x = __uint_as_float(v[j]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j) : 0.f);
+                        q.y = __uint_as_float(v[j + 1]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 1) : 0.f);
+                        q.z = __uint_as_float(v[j + 2]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 2) : 0.f);
+                        q.w = __uint_as_float(v[j + 3]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 3) : 0.f);
+                        *reinterpret_cast<float4*>(o + j) = q;
+                    }
+                } else {
+                    __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(g.out) + row;
+                    for (int j = 0; j < nv; j += 8) {
+                        float y[8];
+                        if (MODE == EPI_BIAS_GELU) {
+                            float z[8];
+#pragma unroll
+                            for (int t = 0; t < 8; ++t) {
+                                z[t] = __uint_as_float(v[j + t]) + __ldg(g.bias + nb + j + t);
+                                y[t] = gelu(z[t]);
+                            }
+                            float* o2 = reinterpret_cast<float*>(g.out2) + row + j;
+                            *reinterpret_cast<float4*>(o2) = make_float4(z[0], z[1], z[2], z[3]);
+                            *reinterpret_cast<float4*>(o2 + 4) = make_float4(z[4], z[5], z[6], z[7]);
+                        } else {  // EPI_DGELU
+                            const float4 a0 = __ldg(reinterpret_cast<const float4*>(g.aux + row + j));
+                            const float4 a1 = __ldg(reinterpret_cast<const float4*>(g.aux + row + j + 4));
+                            const float zz[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+                            for (int t = 0; t < 8; ++t) y[t] = __uint_as_float(v[j + t]) * dgelu(zz[t]);
+                        }
+                        __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(y[2 * t], y[2 * t + 1]);
+                        *reinterpret_cast<uint4*>(o + j) = *reinterpret_cast<const uint4*>(h);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && (S.abort || !ok)) {
+        // let copies still in flight land before the CTA's shared memory is released
+        for (int kc = max(0, issued - STAGES); kc < issued; ++kc) (void)bar_wait(&S.full[kc % STAGES], (kc / STAGES) & 1);
+        atomicExch(g.err, 1);
+    }
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// element-wise / reduction kernels
+// ---------------------------------------------------------------------------
+// out[c][r] = in[r][c] (bf16), 32 x 32 tiles through shared memory.
+__global__ void k_transpose(int rows, int cols, const uint16_t* __restrict__ in, uint16_t* __restrict__ out) {
+    __shared__ uint16_t t[32][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = blockIdx.y * 32 + k;
+        t[k][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * cols + c] : 0;
+    }
+    __syncthreads();
+    const int r2 = blockIdx.y * 32 + threadIdx.x;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c2 = blockIdx.x * 32 + k;
+        if (c2 < cols && r2 < rows) out[(size_t)c2 * rows + r2] = t[threadIdx.x][k];
+    }
+}
+
+// out[n] += sum over the rows of in[r][n] (bf16 in, fp32 out, zeroed by the caller).
+__global__ void k_colsum(int rows, int cols, const __nv_bfloat16* __restrict__ in, float* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const int r0 = blockIdx.y * 256, r1 = min(rows, r0 + 256);
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(in[(size_t)r * cols + c]);
+    atomicAdd(out + c, s);
+}
+
+// Input rows (fp32, n_in wide) -> bf16 rows padded with zeros to ld columns.
+__global__ void k_pack_input(int rows, int n_in, int ld, const float* __restrict__ x, __nv_bfloat16* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)rows * ld) return;
+    const int r = (int)(i / ld), c = (int)(i % ld);
+    out[i] = __float2bfloat16_rn(c < n_in ? x[(size_t)r * n_in + c] : 0.f);
+}
+
+// Mean-squared-error gradient: g = 2 (pred - target) / (rows * cols) as bf16;
+// loss accumulates sum (pred - target)^2 / (rows * cols).
+__global__ void k_mse_grad(int64_t n, float inv, const float* __restrict__ pred, const float* __restrict__ target,
+                           __nv_bfloat16* __restrict__ g, double* loss) {
+    __shared__ float red[32];
+    float acc = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float d = pred[i] - target[i];
+        g[i] = __float2bfloat16_rn(2.f * d * inv);
+        acc += d * d;
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float a = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (threadIdx.x == 0 && loss) atomicAdd(loss, (double)a * inv);
+    }
+}
+
+struct LayerTab {
+    int n;
+    int64_t off[9];       // start of W_l in the flat parameter vector; off[n] = total
+    int out[8], in[8];    // W_l is out x in (in padded); b_l follows W_l
+    int64_t wbf[8];       // offset of layer l in the bf16 weight copies
+};
+
+// Adam with decoupled weight decay on the FP32 master parameters; refreshes
+// the bf16 weights (out x in) and their transpose (in x out).
+__global__ void k_adam(int64_t n, LayerTab T, float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, __nv_bfloat16* __restrict__ wbf, __nv_bfloat16* __restrict__ wtbf,
+                       float lr, float b1, float b2, float eps, float wd, float c1, float c2) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        int l = 0;
+        while (l + 1 < T.n && i >= T.off[l + 1]) ++l;
+        const int64_t w = i - T.off[l];
+        const int64_t nw = (int64_t)T.out[l] * T.in[l];
+        const float decay = w < nw ? wd : 0.f;
+        const float pi = p[i] - lr * ((mi * c1) / (sqrtf(vi * c2) + eps) + decay * p[i]);
+        p[i] = pi;
+        if (w < nw) {
+            const int r = (int)(w / T.in[l]), c = (int)(w % T.in[l]);
+            const __nv_bfloat16 h = __float2bfloat16_rn(pi);
+            wbf[T.wbf[l] + w] = h;
+            wtbf[T.wbf[l] + (int64_t)c * T.out[l] + r] = h;
+        }
+    }
+}
+
+// bf16 copies of the weights (after a parameter upload).
+__global__ void k_cast_weights(int64_t n, LayerTab T, const float* __restrict__ p, __nv_bfloat16* __restrict__ wbf,
+                               __nv_bfloat16* __restrict__ wtbf) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int l = 0;
+        while (l + 1 < T.n && i >= T.off[l + 1]) ++l;
+        const int64_t w = i - T.off[l];
+        if (w < (int64_t)T.out[l] * T.in[l]) {
+            const int r = (int)(w / T.in[l]), c = (int)(w % T.in[l]);
+            const __nv_bfloat16 h = __float2bfloat16_rn(p[i]);
+            wbf[T.wbf[l] + w] = h;
+            wtbf[T.wbf[l] + (int64_t)c * T.out[l] + r] = h;
+        }
+    }
+}
+
+// Per-row chi-squared of a surrogate curve: flux_j = exp(pred_j * sd_j + mean_j),
+// optionally scaled by the least-squares factor (orchestration.rs:361-401 re_scale).
+__global__ void k_logflux_chisq(int rows, int n, const float* __restrict__ pred, const float* __restrict__ mean,
+                                const float* __restrict__ sd, const double* __restrict__ flux,
+                                const double* __restrict__ ferr, int scale, double* __restrict__ out) {
+    __shared__ double red[3][8];
+    const int r = blockIdx.x;
+    if (r >= rows) return;
+    double sff = 0, sfd = 0, sdd = 0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double f = exp((double)pred[(size_t)r * n + j] * sd[j] + mean[j]);
+        const double w = 1.0 / (ferr[j] * ferr[j]);
+        sff += w * f * f;
+        sfd += w * f * flux[j];
+        sdd += w * flux[j] * flux[j];
+    }
+    for (int o = 16; o; o >>= 1) {
+        sff += __shfl_xor_sync(0xffffffffu, sff, o);
+        sfd += __shfl_xor_sync(0xffffffffu, sfd, o);
+        sdd += __shfl_xor_sync(0xffffffffu, sdd, o);
+    }
+    const int wid = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][wid] = sff;
+        red[1][wid] = sfd;
+        red[2][wid] = sdd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, c = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            a += red[0][k];
+            b += red[1][k];
+            c += red[2][k];
+        }
+        const double s = scale ? (a > 0 ? b / a : 0.0) : 1.0;
+        out[r] = c - 2 * s * b + s * s * a;  // sum w (d - s f)^2
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+thread_local std::string t_err;
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(expr)                                                                                                   \
+    do {                                                                                                           \
+        cudaError_t e_ = (expr);                                                                                   \
+        if (e_ != cudaSuccess) throw Fail(LCB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return LCB_OK;
+    } catch (const Fail& e) {
+        t_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        t_err = e.what();
+        return LCB_ERR_INVALID;
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) throw Fail(LCB_ERR_NO_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+// Tensor map of a row-major bf16 matrix (rows x cols), boxes of 64 columns x 128 rows, 128-byte swizzle.
+CUtensorMap bf16_map(const void* ptr, int64_t rows, int64_t cols) {
+    if (((uintptr_t)ptr & 15) || (cols % 8)) throw Fail(LCB_ERR_INVALID, "GEMM operand: 16-byte alignment and cols % 8 == 0 required");
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)BK, 128u};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Fail(LCB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+constexpr size_t kGemmSmem = sizeof(GemmSmem) + 1024;
+
+template <int MODE>
+void launch_gemm_mode(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, cudaStream_t s) {
+    static cudaError_t attr = cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    CK(attr);
+    dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN);
+    k_gemm<MODE><<<grid, GEMM_THREADS, kGemmSmem, s>>>(ta, tb, g);
+    CK(cudaGetLastError());
+}
+
+void gemm(int mode, int64_t M, int64_t N, int64_t K, const void* A, const void* B, const float* bias, const float* aux,
+          void* out, void* out2, int* err, cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0 || N % 8 || K % 8 || M > INT32_MAX || N > 65535 * (int64_t)BN)
+        throw Fail(LCB_ERR_INVALID, "GEMM sizes: M, N, K > 0 and N, K multiples of 8 required");
+    if (((uintptr_t)out & 15) || (out2 && ((uintptr_t)out2 & 15)) || (aux && ((uintptr_t)aux & 15)))
+        throw Fail(LCB_ERR_INVALID, "GEMM outputs must be 16-byte aligned");
+    if ((mode == EPI_BIAS_GELU || mode == EPI_BIAS_F32) && !bias) throw Fail(LCB_ERR_INVALID, "bias required");
+    if (mode == EPI_BIAS_GELU && !out2) throw Fail(LCB_ERR_INVALID, "pre-activation output required");
+    if (mode == EPI_DGELU && !aux) throw Fail(LCB_ERR_INVALID, "pre-activation input required");
+    if (!err) throw Fail(LCB_ERR_INVALID, "error word required");
+    const CUtensorMap ta = bf16_map(A, M, K), tb = bf16_map(B, N, K);
+    GemmArgs g{(int)M, (int)N, (int)K, bias, aux, out, out2, err};
+    switch (mode) {
+        case EPI_F32: launch_gemm_mode<EPI_F32>(ta, tb, g, s); break;
+        case EPI_BIAS_GELU: launch_gemm_mode<EPI_BIAS_GELU>(ta, tb, g, s); break;
+        case EPI_BIAS_F32: launch_gemm_mode<EPI_BIAS_F32>(ta, tb, g, s); break;
+        case EPI_DGELU: launch_gemm_mode<EPI_DGELU>(ta, tb, g, s); break;
+        default: throw Fail(LCB_ERR_INVALID, "unknown GEMM epilogue mode");
+    }
+}
+
+void transpose(int64_t rows, int64_t cols, const void* in, void* out, cudaStream_t s) {
+    dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+    k_transpose<<<grid, dim3(32, 8), 0, s>>>((int)rows, (int)cols, (const uint16_t*)in, (uint16_t*)out);
+    CK(cudaGetLastError());
+}
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        CK(cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T)));
+    }
+    void free() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+}  // namespace
+
+struct lcb_mlp {
+    int device = 0;
+    int n_in = 0, width = 0, n_hidden = 0, n_out = 0, nl = 0;
+    int64_t max_batch = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<int> out, in;         // per layer (in padded to a multiple of 8)
+    LayerTab tab{};
+    int64_t nparam = 0, nwbf = 0;
+    DBuf<float> p, m, v, g;           // flat FP32 parameters [W0 b0 W1 b1 ...], Adam moments, gradients
+    DBuf<__nv_bfloat16> wbf, wtbf;    // bf16 weights and transposes
+    DBuf<__nv_bfloat16> x0;           // packed input
+    std::vector<DBuf<__nv_bfloat16>> y;  // hidden activations (bf16)
+    std::vector<DBuf<float>> z;          // hidden pre-activations (fp32)
+    DBuf<float> pred;
+    DBuf<__nv_bfloat16> dz[2], dzt, xt;
+    DBuf<int> err;
+    DBuf<double> loss;
+    int64_t steps = 0;
+
+    const float* W(int l) const { return p.p + tab.off[l]; }
+    const float* b(int l) const { return p.p + tab.off[l] + (int64_t)out[l] * in[l]; }
+    float* gW(int l) { return g.p + tab.off[l]; }
+    float* gb(int l) { return g.p + tab.off[l] + (int64_t)out[l] * in[l]; }
+
+    void release() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        p.free(); m.free(); v.free(); g.free(); wbf.free(); wtbf.free(); x0.free(); pred.free(); dzt.free(); xt.free();
+        dz[0].free(); dz[1].free(); err.free(); loss.free();
+        for (auto& t : y) t.free();
+        for (auto& t : z) t.free();
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+
+    void check_err() {
+        int h = 0;
+        CK(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (h) throw Fail(LCB_ERR_DEVICE_CHECK, "a bounded wait in the surrogate GEMM timed out");
+    }
+
+    void forward(const float* x, int64_t B, float* y_out) {
+        if (B <= 0 || B > max_batch) throw Fail(LCB_ERR_INVALID, "batch size out of range");
+        const int64_t nx = B * in[0];
+        k_pack_input<<<(unsigned)((nx + 255) / 256), 256, 0, stream>>>((int)B, n_in, in[0], x, x0.p);
+        CK(cudaGetLastError());
+        const void* a = x0.p;
+        for (int l = 0; l < nl; ++l) {
+            if (l + 1 < nl) {
+                gemm(EPI_BIAS_GELU, B, out[l], in[l], a, wbf.p + tab.wbf[l], b(l), nullptr, y[l].p, z[l].p, err.p, stream);
+                a = y[l].p;
+            } else {
+                gemm(EPI_BIAS_F32, B, out[l], in[l], a, wbf.p + tab.wbf[l], b(l), nullptr, y_out ? y_out : pred.p,
+                     nullptr, err.p, stream);
+            }
+        }
+    }
+
+    void backward(const float* x, const float* target, int64_t B) {
+        if (B % 8) throw Fail(LCB_ERR_INVALID, "training batch must be a multiple of 8");
+        forward(x, B, nullptr);
+        const int64_t npred = B * n_out;
+        CK(cudaMemsetAsync(g.p, 0, nparam * sizeof(float), stream));
+        k_mse_grad<<<(unsigned)std::min<int64_t>((npred + 255) / 256, 1184), 256, 0, stream>>>(
+            npred, 1.0f / (float)npred, pred.p, target, dz[0].p, loss.p);
+        CK(cudaGetLastError());
+        int cur = 0;
+        for (int l = nl - 1; l >= 0; --l) {
+            const void* xl = l == 0 ? (const void*)x0.p : (const void*)y[l - 1].p;
+            transpose(B, out[l], dz[cur].p, dzt.p, stream);
+            transpose(B, in[l], xl, xt.p, stream);
+            gemm(EPI_F32, out[l], in[l], B, dzt.p, xt.p, nullptr, nullptr, gW(l), nullptr, err.p, stream);
+            dim3 cg((unsigned)((out[l] + 127) / 128), (unsigned)((B + 255) / 256));
+            k_colsum<<<cg, 128, 0, stream>>>((int)B, out[l], dz[cur].p, gb(l));
+            CK(cudaGetLastError());
+            if (l > 0) {
+                gemm(EPI_DGELU, B, in[l], out[l], dz[cur].p, wtbf.p + tab.wbf[l], nullptr, z[l - 1].p, dz[cur ^ 1].p,
+                     nullptr, err.p, stream);
+                cur ^= 1;
+            }
+        }
+    }
+
+    void adam(float lr, float b1, float b2, float eps, float wd) {
+        ++steps;
+        const float c1 = 1.0f / (1.0f - std::pow(b1, (float)steps)), c2 = 1.0f / (1.0f - std::pow(b2, (float)steps));
+        k_adam<<<(unsigned)std::min<int64_t>((nparam + 255) / 256, 2368), 256, 0, stream>>>(
+            nparam, tab, p.p, m.p, v.p, g.p, wbf.p, wtbf.p, lr, b1, b2, eps, wd, c1, c2);
+        CK(cudaGetLastError());
+    }
+
+    void refresh_bf16() {
+        k_cast_weights<<<(unsigned)std::min<int64_t>((nparam + 255) / 256, 2368), 256, 0, stream>>>(nparam, tab, p.p,
+                                                                                                   wbf.p, wtbf.p);
+        CK(cudaGetLastError());
+    }
+};
+
+extern "C" {
+
+const char* lcb_mlp_last_error(void) { return t_err.c_str(); }
+
+int lcb_mlp_create(int device, int n_in, int width, int n_hidden, int n_out, int64_t max_batch, uint64_t seed,
+                   lcb_mlp** out) {
+    if (!out) return LCB_ERR_INVALID;
+    *out = nullptr;
+    return guard([&] {
+        if (n_in <= 0 || width <= 0 || width % 8 || n_hidden < 1 || n_hidden > 7 || n_out <= 0 || n_out % 8 ||
+            max_batch <= 0 || max_batch > (1 << 24))
+            throw Fail(LCB_ERR_INVALID, "bad network shape (width and n_out multiples of 8, 1..7 hidden layers)");
+        auto N = std::make_unique<lcb_mlp>();
+        N->device = device;
+        CK(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10) throw Fail(LCB_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+        N->n_in = n_in; N->width = width; N->n_hidden = n_hidden; N->n_out = n_out;
+        N->nl = n_hidden + 1;
+        N->max_batch = (max_batch + 7) / 8 * 8;
+        for (int l = 0; l < N->nl; ++l) {
+            N->in.push_back(l == 0 ? (n_in + 7) / 8 * 8 : width);
+            N->out.push_back(l + 1 < N->nl ? width : n_out);
+        }
+        LayerTab& T = N->tab;
+        T.n = N->nl;
+        int64_t off = 0, wo = 0;
+        for (int l = 0; l < N->nl; ++l) {
+            T.off[l] = off;
+            T.out[l] = N->out[l];
+            T.in[l] = N->in[l];
+            T.wbf[l] = wo;
+            off += (int64_t)N->out[l] * N->in[l] + N->out[l];
+            wo += (int64_t)N->out[l] * N->in[l];
+        }
+        T.off[N->nl] = off;
+        N->nparam = off;
+        N->nwbf = wo;
+        CK(cudaStreamCreateWithFlags(&N->stream, cudaStreamNonBlocking));
+        N->own_stream = true;
+        N->p.alloc(off); N->m.alloc(off); N->v.alloc(off); N->g.alloc(off);
+        N->wbf.alloc(wo); N->wtbf.alloc(wo);
+        const int64_t B = N->max_batch;
+        N->x0.alloc(B * N->in[0]);
+        N->y.resize(N->nl - 1);
+        N->z.resize(N->nl - 1);
+        for (int l = 0; l + 1 < N->nl; ++l) {
+            N->y[l].alloc(B * width);
+            N->z[l].alloc(B * width);
+        }
+        const int wmax = std::max(width, n_out);
+        N->pred.alloc(B * n_out);
+        N->dz[0].alloc(B * wmax);
+        N->dz[1].alloc(B * wmax);
+        N->dzt.alloc(B * wmax);
+        N->xt.alloc(B * std::max(width, N->in[0]));
+        N->err.alloc(1);
+        N->loss.alloc(1);
+        // He-uniform initial weights, zero biases (padding columns stay zero)
+        std::vector<float> h(off, 0.f);
+        std::mt19937_64 rng(seed);
+        for (int l = 0; l < N->nl; ++l) {
+            const int fan_in = l == 0 ? n_in : width;
+            const float a = std::sqrt(6.0f / (float)fan_in);
+            std::uniform_real_distribution<float> U(-a, a);
+            for (int r = 0; r < N->out[l]; ++r)
+                for (int c = 0; c < fan_in; ++c) h[T.off[l] + (int64_t)r * N->in[l] + c] = U(rng);
+        }
+        CK(cudaMemcpy(N->p.p, h.data(), off * sizeof(float), cudaMemcpyHostToDevice));
+        N->refresh_bf16();
+        CK(cudaStreamSynchronize(N->stream));
+        *out = N.release();
+    });
+}
+
+void lcb_mlp_destroy(lcb_mlp* net) {
+    if (!net) return;
+    net->release();
+    delete net;
+}
+
+int lcb_mlp_set_stream(lcb_mlp* net, void* stream) {
+    if (!net) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        CK(cudaStreamSynchronize(net->stream));
+        if (net->own_stream) CK(cudaStreamDestroy(net->stream));
+        net->own_stream = stream == nullptr;
+        if (stream) net->stream = (cudaStream_t)stream;
+        else CK(cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking));
+    });
+}
+
+int lcb_mlp_num_params(const lcb_mlp* net, int64_t* n) {
+    if (!net || !n) return LCB_ERR_INVALID;
+    int64_t t = 0;
+    for (int l = 0; l < net->nl; ++l) t += (int64_t)net->out[l] * ((l == 0 ? net->n_in : net->width) + 1);
+    *n = t;
+    return LCB_OK;
+}
+
+// Copies between the unpadded host layout [W0 (out x n_in), b0, W1, b1, ...] and the device layout.
+static void host_layout(const lcb_mlp* net, const float* dev_flat, float* host, bool to_host, std::vector<float>& dev) {
+    int64_t h = 0;
+    for (int l = 0; l < net->nl; ++l) {
+        const int fan = l == 0 ? net->n_in : net->width;
+        for (int r = 0; r < net->out[l]; ++r)
+            for (int c = 0; c < fan; ++c, ++h) {
+                float& d = dev[net->tab.off[l] + (int64_t)r * net->in[l] + c];
+                if (to_host) host[h] = d;
+                else d = host[h];
+            }
+        for (int r = 0; r < net->out[l]; ++r, ++h) {
+            float& d = dev[net->tab.off[l] + (int64_t)net->out[l] * net->in[l] + r];
+            if (to_host) host[h] = d;
+            else d = host[h];
+        }
+    }
+    (void)dev_flat;
+}
+
+static int fetch_flat(lcb_mlp* net, const float* src, float* host, int64_t n) {
+    return guard([&] {
+        int64_t want = 0;
+        lcb_mlp_num_params(net, &want);
+        if (n != want) throw Fail(LCB_ERR_INVALID, "parameter count mismatch");
+        CK(cudaSetDevice(net->device));
+        net->check_err();
+        std::vector<float> dev(net->nparam);
+        CK(cudaMemcpyAsync(dev.data(), src, net->nparam * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaStreamSynchronize(net->stream));
+        host_layout(net, src, host, true, dev);
+    });
+}
+
+int lcb_mlp_get_params(lcb_mlp* net, float* host, int64_t n) {
+    if (!net || !host) return LCB_ERR_INVALID;
+    return fetch_flat(net, net->p.p, host, n);
+}
+
+int lcb_mlp_get_grads(lcb_mlp* net, float* host, int64_t n) {
+    if (!net || !host) return LCB_ERR_INVALID;
+    return fetch_flat(net, net->g.p, host, n);
+}
+
+int lcb_mlp_set_params(lcb_mlp* net, const float* host, int64_t n) {
+    if (!net || !host) return LCB_ERR_INVALID;
+    return guard([&] {
+        int64_t want = 0;
+        lcb_mlp_num_params(net, &want);
+        if (n != want) throw Fail(LCB_ERR_INVALID, "parameter count mismatch");
+        CK(cudaSetDevice(net->device));
+        std::vector<float> dev(net->nparam, 0.f);
+        host_layout(net, nullptr, const_cast<float*>(host), false, dev);
+        CK(cudaMemcpyAsync(net->p.p, dev.data(), net->nparam * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+        CK(cudaMemsetAsync(net->m.p, 0, net->nparam * sizeof(float), net->stream));
+        CK(cudaMemsetAsync(net->v.p, 0, net->nparam * sizeof(float), net->stream));
+        net->steps = 0;
+        net->refresh_bf16();
+        CK(cudaStreamSynchronize(net->stream));
+    });
+}
+
+int lcb_mlp_forward(lcb_mlp* net, const float* x_dev, int64_t batch, float* y_dev) {
+    if (!net || !x_dev || !y_dev) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->forward(x_dev, batch, y_dev);
+    });
+}
+
+int lcb_mlp_backward(lcb_mlp* net, const float* x_dev, const float* target_dev, int64_t batch) {
+    if (!net || !x_dev || !target_dev) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->backward(x_dev, target_dev, batch);
+    });
+}
+
+int lcb_mlp_train_step(lcb_mlp* net, const float* x_dev, const float* target_dev, int64_t batch, float lr,
+                       float beta1, float beta2, float eps, float weight_decay) {
+    if (!net || !x_dev || !target_dev) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->backward(x_dev, target_dev, batch);
+        net->adam(lr, beta1, beta2, eps, weight_decay);
+    });
+}
+
+int lcb_mlp_take_loss(lcb_mlp* net, double* loss_sum) {
+    if (!net || !loss_sum) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->check_err();
+        CK(cudaMemcpyAsync(loss_sum, net->loss.p, sizeof(double), cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaMemsetAsync(net->loss.p, 0, sizeof(double), net->stream));
+        CK(cudaStreamSynchronize(net->stream));
+    });
+}
+
+int lcb_mlp_sync(lcb_mlp* net) {
+    if (!net) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->check_err();
+    });
+}
+
+int lcb_mlp_gemm(int mode, int64_t M, int64_t N, int64_t K, const void* a, const void* b, const float* bias,
+                 const float* aux, void* out, void* out2, int* err_dev, void* stream) {
+    return guard([&] { gemm(mode, M, N, K, a, b, bias, aux, out, out2, err_dev, (cudaStream_t)stream); });
+}
+
+int lcb_logflux_chisq(int64_t rows, int n, const float* pred, const float* mean, const float* sd, const double* flux,
+                      const double* ferr, int scale, double* chisq_out, void* stream) {
+    if (rows <= 0 || n <= 0 || !pred || !mean || !sd || !flux || !ferr || !chisq_out) return LCB_ERR_INVALID;
+    return guard([&] {
+        k_logflux_chisq<<<(unsigned)rows, 128, 0, (cudaStream_t)stream>>>((int)rows, n, pred, mean, sd, flux, ferr,
+                                                                          scale, chisq_out);
+        CK(cudaGetLastError());
+    });
+}
+
+}  // extern "C"

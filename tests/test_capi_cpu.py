@@ -9,7 +9,7 @@ from conftest import GOLDEN, ROOT
 
 
 def header_symbols():
-    text = (ROOT / "include" / "lcurve_b200.h").read_text()
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
     return sorted(set(re.findall(r"\b(lcb_[a-z_0-9]+)\s*\(", text)))
 
 
