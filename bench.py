@@ -14,6 +14,13 @@ data (lcurve-rs_b200/workloads.py).
           pinned host memory: host planning, H2D of tables and data, kernels,
           D2H of the results, every step.
 
+  mcmc  : (1 GPU) the surrogate pipeline -- light curves generated by the
+          engine, the BF16 tensor-core MLP trained on them, then 256-walker
+          delayed-acceptance MCMC against plain engine MCMC from one burned-in
+          ensemble: ESS/s of each, surrogate error, posterior agreement.
+          Defaults are a reduced run (524k curves, 2000 steps); --mcmc-full
+          runs the full 1M-curve, 20000-step configuration.
+
 Multi-GPU (torchrun): weak scaling, each rank evaluates its own 1024-model
 batch (seed 1234 + rank); no collective on the data path, only the timing
 reduction.  `--impl reference` times the CPU oracle (the FP64 restatement of
@@ -35,7 +42,7 @@ import numpy as np
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "model evals/s (1024-model batch)"
+METRIC = "model evals/s (1024-model batch) & MCMC ESS/s, surrogate-DA vs plain"
 UNIT = "model evals/s"
 FLUX_FLOPS_PER_EVAL = 17     # dot 5 + limb darkening 9 + product 2 + accumulate 1
 POT_FLOPS_PER_EVAL = 22      # one Roche potential (or gradient) evaluation
@@ -51,7 +58,19 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=0, help="models per CPU-baseline step (0 = host threads)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    return p.parse_args()
+    # surrogate delayed-acceptance MCMC (256 walkers; 1 GPU)
+    p.add_argument("--no-mcmc", action="store_true")
+    p.add_argument("--mcmc-full", action="store_true",
+                   help="full size: 1M training curves, 300 epochs, 20000 steps")
+    p.add_argument("--mcmc-curves", type=int, default=524288)
+    p.add_argument("--mcmc-epochs", type=int, default=250)
+    p.add_argument("--mcmc-steps", type=int, default=2000)
+    p.add_argument("--mcmc-burn", type=int, default=500)
+    p.add_argument("--mcmc-substeps", type=int, default=32)
+    a = p.parse_args()
+    if a.mcmc_full:
+        a.mcmc_curves, a.mcmc_epochs, a.mcmc_steps = 1048576, 300, 20000
+    return a
 
 
 class ClockSampler:
@@ -166,6 +185,10 @@ def run_reference(args, rank, world):
         if s >= args.warmup:
             rates.append(r)
     v = float(np.mean(rates))
+    mcmc = None
+    if world == 1 and not args.no_mcmc:
+        mcmc = run_mcmc(args, lcb)
+
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak",
@@ -179,6 +202,62 @@ def run_reference(args, rank, world):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_mcmc(args, lcb):
+    """Surrogate delayed-acceptance MCMC against plain engine MCMC: 256
+    walkers on the fixed 256-phase problem (fiducial curve + 1% noise), both
+    started from one burned-in ensemble; ESS/s over the sampling loops."""
+    S = importlib.import_module("lcurve-rs_b200.surrogate")
+    M = importlib.import_module("lcurve-rs_b200.mcmc")
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    setup = S.CurveSetup()
+    n, hold = args.mcmc_curves, 4096
+    t0 = time.perf_counter()
+    theta = S.sample_prior(n + hold, seed=1)
+    curves = S.generate_curves(setup, theta)
+    gen_s = time.perf_counter() - t0
+    sur = S.Surrogate()
+    losses = sur.fit(theta[:n], curves[:n], epochs=args.mcmc_epochs)
+    ok = np.isfinite(curves[n:]).all(axis=1)
+    rel = S.scaled_rel_error(sur.predict(theta[n:][ok]), curves[n:][ok])
+
+    fid = S.CurveEngine(setup).curves(S.TRUTH[None, :])[0]
+    data = W.noisy_data(setup.times, fid, setup.expose, setup.ndiv, seed=42)
+    eng = S.CurveEngine(setup, data=data)
+    sur.bind_data(data)
+    p0 = M.initial_walkers(256, S.TRUTH, seed=3)
+    burn = M.run_delayed(eng, sur, p0, args.mcmc_burn, seed=4, substeps=args.mcmc_substeps)
+    start = burn.chain[-1]
+    plain = M.run_plain(eng, start, args.mcmc_steps, seed=5)
+    da = M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=args.mcmc_substeps)
+    ess_p, tau_p = M.ess(plain, burn=0.0)
+    ess_d, tau_d = M.ess(da, burn=0.0)
+    post = plain.chain[-1][:128]
+    dchi = eng.chisq(post) - sur.chisq(post)
+    sp, sd = M.posterior_summary(plain, burn=0.0), M.posterior_summary(da, burn=0.0)
+    shift = max(abs(sd[k][0] - sp[k][0]) / sp[k][1] for k in sp)
+    return {
+        "ess_per_s_plain": ess_p / plain.seconds, "ess_per_s_da": ess_d / da.seconds,
+        "speedup": (ess_d / da.seconds) / (ess_p / plain.seconds),
+        "ess_per_s_da_incl_training": ess_d / (da.seconds + gen_s + sur.train_seconds),
+        "ess": {"plain": ess_p, "da": ess_d}, "tau": {"plain": tau_p.tolist(), "da": tau_d.tolist()},
+        "seconds": {"plain": plain.seconds, "da": da.seconds, "curve_generation": gen_s,
+                    "training": sur.train_seconds, "burn_in": burn.seconds},
+        "engine_evals": {"plain": plain.engine_evals, "da": da.engine_evals},
+        "surrogate_evals_da": da.surrogate_evals,
+        "acceptance": {"plain": plain.acceptance, "da": da.acceptance},
+        "posterior": {"plain": sp, "da": sd, "max_mean_shift_in_plain_sigma": shift},
+        "surrogate": {"network": "5 -> 4 x 512 (GELU) -> 256, BF16 tcgen05 kernels, FP32 accumulation",
+                      "train_curves": n, "epochs": args.mcmc_epochs, "final_loss": losses[-1],
+                      "holdout_scaled_rel_err": {"median": float(np.median(rel)),
+                                                 "p99": float(np.quantile(rel, 0.99)), "max": float(rel.max())},
+                      "posterior_chisq_minus_engine": {"mean": float(-dchi.mean()), "std": float(dchi.std())}},
+        "config": {"walkers": 256, "steps": args.mcmc_steps, "burn_in_steps": args.mcmc_burn,
+                   "substeps": args.mcmc_substeps, "phases": setup.n_phase, "stretch_a": 2.0,
+                   "likelihood": "-chisq/2, chisq_batch scale=True, uniform prior box of the 1024-model batch",
+                   "data": "fiducial single_small curve at 256 phases + 1% Gaussian noise, seed 42"},
+    }
 
 
 def main():
@@ -304,6 +383,10 @@ def main():
                "sample": f"first {sample} models of the batch, all host threads, parallel over models "
                          "(oracle/lcurve_oracle.cpp, FP64 restatement of the reference CPU path)"}
 
+    mcmc = None
+    if world == 1 and not args.no_mcmc:
+        mcmc = run_mcmc(args, lcb)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -322,6 +405,7 @@ def main():
         "e2e": e2e,
         "gpu_launches": 6 * args.steps,
         "clocks": clk.summary(),
+        "mcmc": mcmc if mcmc is not None else {"skipped": "multi-GPU run or --no-mcmc; the MCMC comparison runs on 1 GPU"},
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -50,6 +50,7 @@ SYMBOLS = [
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
     "lcb_mlp_train_step", "lcb_mlp_take_loss", "lcb_mlp_sync", "lcb_mlp_gemm", "lcb_logflux_chisq",
+    "lcb_surrogate_subchain",
 ]
 
 _lib = None
@@ -109,6 +110,8 @@ def load():
         "lcb_mlp_sync": ([vp], i),
         "lcb_mlp_gemm": ([i, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, vp], i),
         "lcb_logflux_chisq": ([i64, i, vp, vp, vp, vp, vp, i, vp, vp], i),
+        "lcb_surrogate_subchain": ([vp, i64, i64, i, vp, vp, vp, vp, i, d, dp, dp, C.POINTER(i),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, vp, vp, i], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -423,6 +423,66 @@ __global__ void k_logflux_chisq(int rows, int n, const float* __restrict__ pred,
 }
 
 // ---------------------------------------------------------------------------
+// surrogate sub-chain: stretch moves under the surrogate posterior, on device
+// ---------------------------------------------------------------------------
+constexpr int kMaxDim = 8;
+
+struct StretchArgs {
+    int n, m, d, n_in;
+    double* y;             // n x d sub-chain positions (in/out)
+    double* ls;            // n surrogate log probabilities (in/out)
+    const double* comp;    // m x d complementary walkers (fixed)
+    const double* rnd;     // K x n x 3: uniform for z, uniform for the partner, log uniform for acceptance
+    double* yp;            // n x d proposals
+    double* lz;            // n: (d - 1) ln z, or -inf outside the prior box
+    float* xin;            // n x n_in network inputs
+    double lo[kMaxDim], hi[kMaxDim];
+    float fmul[kMaxDim], fadd[kMaxDim];
+    int frecip[kMaxDim];
+    double a;
+};
+
+// Goodman & Weare stretch proposal y' = c + z (y - c), z ~ g(z) on [1/a, a];
+// the network input of y' is fadd + fmul * (y' or 1/y') per dimension.
+__global__ void k_stretch_propose(StretchArgs A, int step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const double* r = A.rnd + ((size_t)step * A.n + i) * 3;
+    // explicitly rounded operations (no contraction), so the moves are the
+    // ones a host implementation of the same formulas makes
+    double z = __dadd_rn(__dmul_rn(A.a - 1.0, r[0]), 1.0);
+    z = __ddiv_rn(__dmul_rn(z, z), A.a);
+    const int j = min((int)(r[1] * A.m), A.m - 1);
+    bool inside = true;
+    for (int k = 0; k < A.d; ++k) {
+        const double c = A.comp[(size_t)j * A.d + k];
+        const double v = __dadd_rn(c, __dmul_rn(z, __dsub_rn(A.y[(size_t)i * A.d + k], c)));
+        A.yp[(size_t)i * A.d + k] = v;
+        inside = inside && v >= A.lo[k] && v <= A.hi[k];
+        const double f = A.frecip[k] ? 1.0 / v : v;
+        // separate multiply and add (no contraction): the host computes the inputs the same way
+        A.xin[(size_t)i * A.n_in + k] = (float)__dadd_rn((double)A.fadd[k], __dmul_rn((double)A.fmul[k], f));
+    }
+    A.lz[i] = inside ? (A.d - 1) * log(z) : -INFINITY;
+}
+
+// Metropolis step of the sub-chain: accept y' with min(1, z^(d-1) exp(l~(y') - l~(y))),
+// l~ = -chisq / 2 inside the prior box.
+__global__ void k_stretch_accept(StretchArgs A, const double* __restrict__ chi, int step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const double lz = A.lz[i];
+    if (lz == -INFINITY) return;
+    double lsp = -0.5 * chi[i];
+    if (!(lsp == lsp)) lsp = -INFINITY;
+    const double logu = A.rnd[((size_t)step * A.n + i) * 3 + 2];
+    if (logu < lz + lsp - A.ls[i]) {
+        for (int k = 0; k < A.d; ++k) A.y[(size_t)i * A.d + k] = A.yp[(size_t)i * A.d + k];
+        A.ls[i] = lsp;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 thread_local std::string t_err;
@@ -554,6 +614,8 @@ struct lcb_mlp {
     DBuf<__nv_bfloat16> dz[2], dzt, xt;
     DBuf<int> err;
     DBuf<double> loss;
+    DBuf<float> sub_x;                   // sub-chain: network inputs
+    DBuf<double> sub_yp, sub_lz, sub_chi;  // proposals, (d-1) ln z, chi-squared
     int64_t steps = 0;
 
     const float* W(int l) const { return p.p + tab.off[l]; }
@@ -566,6 +628,7 @@ struct lcb_mlp {
         if (stream) cudaStreamSynchronize(stream);
         p.free(); m.free(); v.free(); g.free(); wbf.free(); wtbf.free(); x0.free(); pred.free(); dzt.free(); xt.free();
         dz[0].free(); dz[1].free(); err.free(); loss.free();
+        sub_x.free(); sub_yp.free(); sub_lz.free(); sub_chi.free();
         for (auto& t : y) t.free();
         for (auto& t : z) t.free();
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -695,6 +758,10 @@ int lcb_mlp_create(int device, int n_in, int width, int n_hidden, int n_out, int
         N->xt.alloc(B * std::max(width, N->in[0]));
         N->err.alloc(1);
         N->loss.alloc(1);
+        N->sub_x.alloc(B * N->in[0]);
+        N->sub_yp.alloc(B * kMaxDim);
+        N->sub_lz.alloc(B);
+        N->sub_chi.alloc(B);
         // He-uniform initial weights, zero biases (padding columns stay zero)
         std::vector<float> h(off, 0.f);
         std::mt19937_64 rng(seed);
@@ -848,6 +915,41 @@ int lcb_mlp_sync(lcb_mlp* net) {
 int lcb_mlp_gemm(int mode, int64_t M, int64_t N, int64_t K, const void* a, const void* b, const float* bias,
                  const float* aux, void* out, void* out2, int* err_dev, void* stream) {
     return guard([&] { gemm(mode, M, N, K, a, b, bias, aux, out, out2, err_dev, (cudaStream_t)stream); });
+}
+
+int lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y_dev, double* ls_dev,
+                           const double* comp_dev, const double* rnd_dev, int steps, double a, const double* lo,
+                           const double* hi, const int* recip, const float* fmul, const float* fadd,
+                           const float* mean_dev, const float* sd_dev, const double* flux_dev, const double* ferr_dev,
+                           int scale) {
+    if (!net || !y_dev || !ls_dev || !comp_dev || !rnd_dev || !lo || !hi || !recip || !fmul || !fadd || !mean_dev ||
+        !sd_dev || !flux_dev || !ferr_dev)
+        return LCB_ERR_INVALID;
+    return guard([&] {
+        if (n <= 0 || n > net->max_batch || m <= 0 || m > INT32_MAX || d != net->n_in || d > kMaxDim || steps < 0 ||
+            !(a > 1.0))
+            throw Fail(LCB_ERR_INVALID, "sub-chain: 0 < n <= max_batch, d == n_in <= 8, a > 1 required");
+        CK(cudaSetDevice(net->device));
+        StretchArgs A{};
+        A.n = (int)n; A.m = (int)m; A.d = d; A.n_in = net->n_in;  // rows of lcb_mlp_forward input: n_in wide
+        A.y = y_dev; A.ls = ls_dev; A.comp = comp_dev; A.rnd = rnd_dev;
+        A.yp = net->sub_yp.p; A.lz = net->sub_lz.p; A.xin = net->sub_x.p;
+        for (int k = 0; k < d; ++k) {
+            A.lo[k] = lo[k]; A.hi[k] = hi[k]; A.frecip[k] = recip[k]; A.fmul[k] = fmul[k]; A.fadd[k] = fadd[k];
+        }
+        A.a = a;
+        const unsigned g = (unsigned)((n + 127) / 128);
+        for (int k = 0; k < steps; ++k) {
+            k_stretch_propose<<<g, 128, 0, net->stream>>>(A, k);
+            CK(cudaGetLastError());
+            net->forward(net->sub_x.p, n, nullptr);
+            k_logflux_chisq<<<(unsigned)n, 128, 0, net->stream>>>((int)n, net->n_out, net->pred.p, mean_dev, sd_dev,
+                                                                 flux_dev, ferr_dev, scale, net->sub_chi.p);
+            CK(cudaGetLastError());
+            k_stretch_accept<<<g, 128, 0, net->stream>>>(A, net->sub_chi.p, k);
+            CK(cudaGetLastError());
+        }
+    });
 }
 
 int lcb_logflux_chisq(int64_t rows, int n, const float* pred, const float* mean, const float* sd, const double* flux,

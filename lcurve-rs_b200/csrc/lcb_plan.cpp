@@ -12,9 +12,11 @@
 #include "lcb_plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <thread>
 
 namespace lcb {
 
@@ -701,18 +703,31 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     P.model_ok.assign(n, 0);
     P.model_err.assign(n, std::string());
     std::vector<ModelLayout> lay(n);
-    for (int64_t i = 0; i < n; ++i) {
+    auto prep = [&](int64_t i) {
         int64_t nd = count[i];
         try {
             if (nd <= 0) throw Error(LCB_ERR_EMPTY, "no data points");
             prepare_model(*models[i], data + start[i], nd, lay[i]);
             P.model_ok[i] = 1;
-        } catch (const Error& e) {
+        } catch (const std::exception& e) {
             P.model_err[i] = e.what();
             lay[i] = ModelLayout();
             std::memset(&lay[i].dev, 0, sizeof(ModelDev));
             lay[i].dev.status = -1;
         }
+    };
+    // models are independent: prepare them on the host's cores (8 or more per thread)
+    const int64_t nthreads = std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), (n + 7) / 8);
+    if (nthreads <= 1) {
+        for (int64_t i = 0; i < n; ++i) prep(i);
+    } else {
+        std::atomic<int64_t> next{0};
+        std::vector<std::thread> pool;
+        for (int64_t t = 0; t < nthreads; ++t)
+            pool.emplace_back([&] {
+                for (int64_t i; (i = next.fetch_add(1)) < n;) prep(i);
+            });
+        for (auto& t : pool) t.join();
     }
     // sub-phases and data
     P.ndatum = 0;
@@ -738,8 +753,10 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     }
     P.nsub = sub;
 
-    // global element / table layout
+    // global element / table layout (a model's segments are contiguous)
+    std::vector<size_t> seg_begin(n + 1);
     for (int64_t i = 0; i < n; ++i) {
+        seg_begin[i] = P.segs.size();
         ModelLayout& L = lay[i];
         int32_t band0 = (int32_t)P.bands.size(), ring0 = (int32_t)P.rings.size();
         P.bands.insert(P.bands.end(), L.bands.begin(), L.bands.end());
@@ -753,6 +770,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         }
         P.nelem += L.nelem;
     }
+    seg_begin[n] = P.segs.size();
     if (P.nelem > ((int64_t)1 << 34)) throw Error(LCB_ERR_INVALID, "batch too large (elements)");
 
     // element-kernel blocks; Roche ray-march blocks (one per eclipsing Roche star); star-grid aux blocks
@@ -804,9 +822,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             return (int32_t)(UK_STAR_POLY1 + (np - 1));
         };
         for (int pass = 0; pass < 3; ++pass) {  // star1 slots, star2 slots, the rest
-            for (size_t s = 0; s < P.segs.size(); ++s) {
+            for (size_t s = seg_begin[i]; s < seg_begin[i + 1]; ++s) {
                 const SegDesc& g = P.segs[s];
-                if (g.model != i) continue;
                 int grp = g.kind == SEG_STAR1 ? 0 : g.kind == SEG_STAR2 ? 1 : 2;
                 if (grp != pass) continue;
                 for (int64_t e = 0; e < g.count; e += erange) {

@@ -1,0 +1,230 @@
+"""Affine-invariant ensemble MCMC over the light-curve likelihood, plain and
+with surrogate delayed acceptance.
+
+The plain sampler is the reference fitter's emcee run
+(python/lcurve_rs/fitting.py:536-600): walkers move by the stretch move
+(Goodman & Weare 2010, a = 2) in two halves, each half's proposals evaluated
+as one batch; log probability = log prior (uniform box) - chisq / 2 with
+chisq from the light-curve engine (chisq_batch with scale=True,
+fitting.py:329-341).
+
+The delayed-acceptance sampler (Christen & Fox 2005) screens moves with
+the surrogate first.  Each half-step, every walker of the moving half runs
+`substeps` stretch moves against the (fixed) other half under the surrogate
+posterior alone,
+
+  stage 1  each sub-step accepted with min(1, z^(d-1) exp(l~(y) - l~(x)))
+           l~ = surrogate log probability,
+
+which is a kernel reversible with respect to the surrogate posterior; only a
+walker whose sub-chain moved it from x to y is then judged by the engine,
+
+  stage 2  accept y with min(1, exp(l(y) - l(x) - l~(y) + l~(x)))
+           l = engine log probability,
+
+else it stays at x.  With substeps = 1 this is Christen & Fox's two-stage
+delayed acceptance; with more sub-steps it is the surrogate transition method
+(Liu 2001, sec. 9.4.3).  Either way the pair of stages satisfies detailed
+balance with respect to the engine's posterior, so both samplers target the
+same distribution and the engine judges every accepted move.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+
+import numpy as np
+
+from .surrogate import PARAMS, PRIOR_HI, PRIOR_LO
+
+
+def log_prior(theta: np.ndarray) -> np.ndarray:
+    theta = np.atleast_2d(theta)
+    inside = np.all((theta >= PRIOR_LO) & (theta <= PRIOR_HI), axis=1)
+    return np.where(inside, 0.0, -np.inf)
+
+
+def _loglike(chisq: np.ndarray) -> np.ndarray:
+    ll = -0.5 * np.asarray(chisq, dtype=np.float64)
+    ll[~np.isfinite(ll)] = -np.inf
+    return ll
+
+
+def _stretch(rng, xs, xc, a):
+    """Stretch proposals for the walkers xs against the complementary half xc."""
+    n, d = xs.shape
+    z = ((a - 1.0) * rng.random(n) + 1.0) ** 2 / a
+    j = rng.integers(0, xc.shape[0], n)
+    return xc[j] + z[:, None] * (xs - xc[j]), z
+
+
+def subchain_numbers(rng, steps: int, n: int) -> np.ndarray:
+    """steps x n x 3 random numbers of a surrogate sub-chain: a uniform for the
+    stretch factor, a uniform for the partner, ln of a uniform for acceptance."""
+    r = rng.random((steps, n, 3))
+    with np.errstate(divide="ignore"):
+        r[..., 2] = np.log(r[..., 2])
+    return r
+
+
+def subchain_host(surrogate, y, ls, comp, rnd, a=2.0):
+    """The surrogate sub-chain on the host, one surrogate call per move; the
+    same arithmetic as the device sub-chain (lcb_surrogate_subchain)."""
+    y, ls = y.copy(), ls.copy()
+    n, d = y.shape
+    m = comp.shape[0]
+    for r in rnd:
+        z = ((a - 1.0) * r[:, 0] + 1.0) ** 2 / a
+        j = np.minimum((r[:, 1] * m).astype(np.int64), m - 1)
+        yp = comp[j] + z[:, None] * (y - comp[j])
+        prior = log_prior(yp)
+        lsp = prior + _loglike(surrogate.chisq(yp, scale=True))
+        take = np.isfinite(prior) & (r[:, 2] < (d - 1) * np.log(z) + lsp - ls)
+        y[take] = yp[take]
+        ls[take] = lsp[take]
+    return y, ls
+
+
+@dataclasses.dataclass
+class Run:
+    chain: np.ndarray            # (nsteps, nwalkers, ndim)
+    seconds: float               # wall time of the sampling loop
+    engine_evals: int            # light curves computed by the engine
+    surrogate_evals: int = 0
+    stage1_pass: int = 0
+    proposals: int = 0
+    accepted: int = 0
+
+    @property
+    def acceptance(self) -> float:
+        return self.accepted / max(self.proposals, 1)
+
+
+def _eval_engine(engine, theta, chunk=128):
+    out = np.full(theta.shape[0], -np.inf)
+    for i in range(0, theta.shape[0], chunk):
+        out[i:i + chunk] = _loglike(engine.chisq(theta[i:i + chunk], scale=True))
+    return out
+
+
+def _eval_prob(engine, theta):
+    lp = log_prior(theta)
+    ok = np.isfinite(lp)
+    out = np.full(theta.shape[0], -np.inf)
+    if ok.any():
+        out[ok] = lp[ok] + _eval_engine(engine, theta[ok])
+    return out
+
+
+def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0) -> Run:
+    rng = np.random.default_rng(seed)
+    x = np.array(p0, dtype=np.float64)
+    nw, d = x.shape
+    half = nw // 2
+    chain = np.empty((nsteps, nw, d))
+    t0 = time.perf_counter()
+    ev0 = engine.evals
+    lp = _eval_prob(engine, x)
+    acc = props = 0
+    for s in range(nsteps):
+        perm = rng.permutation(nw)
+        for h in (0, 1):
+            S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
+            y, z = _stretch(rng, x[S], x[Cc], a)
+            lpy = _eval_prob(engine, y)
+            loga = (d - 1) * np.log(z) + lpy - lp[S]
+            take = np.log(rng.random(len(S))) < loga
+            x[S[take]] = y[take]
+            lp[S[take]] = lpy[take]
+            acc += int(take.sum())
+            props += len(S)
+        chain[s] = x
+    return Run(chain, time.perf_counter() - t0, engine.evals - ev0, proposals=props, accepted=acc)
+
+
+def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0,
+                substeps: int = 1, device_subchain: bool | None = None) -> Run:
+    rng = np.random.default_rng(seed)
+    x = np.array(p0, dtype=np.float64)
+    nw, d = x.shape
+    half = nw // 2
+    chain = np.empty((nsteps, nw, d))
+    t0 = time.perf_counter()
+    ev0 = engine.evals
+    lp = _eval_prob(engine, x)
+    lps = log_prior(x) + _loglike(surrogate.chisq(x, scale=True))
+    on_device = hasattr(surrogate, "subchain") if device_subchain is None else device_subchain
+    acc = props = passed = nsur = 0
+    for s in range(nsteps):
+        perm = rng.permutation(nw)
+        for h in (0, 1):
+            S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
+            # stage 1: a surrogate sub-chain for every walker of the half
+            rnd = subchain_numbers(rng, substeps, len(S))
+            if on_device:
+                y, lsy = surrogate.subchain(x[S], lps[S], x[Cc], rnd, a)
+            else:
+                y, lsy = subchain_host(surrogate, x[S], lps[S], x[Cc], rnd, a)
+            nsur += substeps * len(S)
+            moved = np.any(y != x[S], axis=1)
+            # stage 2: the engine judges the walkers that moved
+            if moved.any():
+                idx = np.nonzero(moved)[0]
+                lpy = log_prior(y[idx]) + _eval_engine(engine, y[idx])
+                loga2 = lpy - lp[S[idx]] - (lsy[idx] - lps[S[idx]])
+                take = np.log(rng.random(len(idx))) < loga2
+                w = S[idx[take]]
+                x[w] = y[idx[take]]
+                lp[w] = lpy[take]
+                lps[w] = lsy[idx[take]]
+                acc += int(take.sum())
+                passed += len(idx)
+            props += len(S)
+        chain[s] = x
+    return Run(chain, time.perf_counter() - t0, engine.evals - ev0, surrogate_evals=nsur, stage1_pass=passed,
+               proposals=props, accepted=acc)
+
+
+# ---------------------------------------------------------------------------
+# effective sample size (integrated autocorrelation time, emcee's estimator)
+# ---------------------------------------------------------------------------
+def _acf(x: np.ndarray) -> np.ndarray:
+    n = len(x)
+    m = 1 << (2 * n - 1).bit_length()
+    f = np.fft.rfft(x - x.mean(), n=m)
+    r = np.fft.irfft(f * np.conj(f), n=m)[:n]
+    return r / r[0] if r[0] > 0 else np.zeros(n)
+
+
+def integrated_time(chain: np.ndarray, c: float = 5.0) -> np.ndarray:
+    """tau per parameter for a (nsteps, nwalkers, ndim) chain: the
+    walker-averaged autocorrelation function summed up to Sokal's automatic
+    window (the smallest M with M >= c tau(M))."""
+    nsteps, nw, d = chain.shape
+    tau = np.empty(d)
+    for k in range(d):
+        f = np.mean([_acf(chain[:, w, k]) for w in range(nw)], axis=0)
+        taus = 2.0 * np.cumsum(f) - 1.0
+        m = np.arange(len(taus)) < c * taus
+        win = int(np.argmin(m)) if not m.all() else len(taus) - 1
+        tau[k] = taus[win]
+    return tau
+
+
+def ess(run: Run, burn: float = 0.25) -> tuple[float, np.ndarray]:
+    """Minimum over parameters of (post-burn samples / tau), and the taus."""
+    ch = run.chain[int(burn * run.chain.shape[0]):]
+    tau = integrated_time(ch)
+    n = ch.shape[0] * ch.shape[1]
+    return float(np.min(n / tau)), tau
+
+
+def posterior_summary(run: Run, burn: float = 0.25) -> dict:
+    ch = run.chain[int(burn * run.chain.shape[0]):].reshape(-1, run.chain.shape[2])
+    return {p: (float(ch[:, i].mean()), float(ch[:, i].std())) for i, p in enumerate(PARAMS)}
+
+
+def initial_walkers(nwalkers: int, center: np.ndarray, seed: int, spread: float = 1e-3) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    p = center + spread * (PRIOR_HI - PRIOR_LO) * rng.standard_normal((nwalkers, len(center)))
+    return np.clip(p, PRIOR_LO, PRIOR_HI)

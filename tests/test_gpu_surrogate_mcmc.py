@@ -1,0 +1,79 @@
+"""What the trained surrogate gains: delayed-acceptance MCMC against plain
+engine MCMC on the 256-phase problem, on the GPU.
+
+* the device sub-chain (lcb_surrogate_subchain) makes the same moves as the
+  host loop that calls the surrogate once per move, on the same random numbers;
+* the surrogate is trained on light curves the engine generates and its error
+  is measured against the engine on held-out parameters;
+* from one burned-in ensemble, delayed acceptance mixes faster per light
+  curve the engine computes and per second than plain MCMC.  Mixing is the
+  mean squared jump of the walkers in units of the plain chain's spread,
+  which is robust on chains too short for autocorrelation times.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods():
+    return (importlib.import_module("lcurve-rs_b200.surrogate"), importlib.import_module("lcurve-rs_b200.mcmc"),
+            importlib.import_module("lcurve-rs_b200.workloads"))
+
+
+def _msjd(run, sig):
+    d = np.diff(run.chain, axis=0) / sig
+    return float(np.mean(np.sum(d * d, axis=2)))
+
+
+def _problem(S, W):
+    setup = S.CurveSetup()
+    fid = S.CurveEngine(setup).curves(S.TRUTH[None, :])[0]
+    data = W.noisy_data(setup.times, fid, setup.expose, setup.ndiv, seed=42)
+    return setup, data
+
+
+def test_device_subchain_matches_host_loop(lcb, mods):
+    S, M, W = mods
+    setup, data = _problem(S, W)
+    sur = S.Surrogate(seed=2)  # untrained weights are enough to compare the two paths
+    sur.bind_data(data)
+    rng = np.random.default_rng(0)
+    walkers = M.initial_walkers(128, S.TRUTH, seed=1, spread=0.05)
+    y, comp = walkers[:64], walkers[64:]
+    ls = -0.5 * sur.chisq(y)
+    rnd = M.subchain_numbers(rng, 6, 64)
+    yd, lsd = sur.subchain(y, ls, comp, rnd)
+    yh, lsh = M.subchain_host(sur, y, ls, comp, rnd)
+    same = np.all(np.isclose(yd, yh, rtol=1e-12, atol=0), axis=1)
+    # identical moves except where float rounding of the network input decides a tie
+    assert same.mean() >= 0.95
+    assert np.allclose(lsd[same], lsh[same], rtol=1e-6, atol=1e-6)
+    assert np.any(np.any(yd != y, axis=1))
+
+
+def test_trained_surrogate_gains_over_plain_mcmc(lcb, mods):
+    S, M, W = mods
+    setup, data = _problem(S, W)
+    n, hold = 393216, 2048
+    theta = S.sample_prior(n + hold, seed=11)
+    curves = S.generate_curves(setup, theta)
+    assert np.isfinite(curves).all()
+    sur = S.Surrogate(seed=1)
+    losses = sur.fit(theta[:n], curves[:n], epochs=250)
+    assert losses[-1] < 0.01 * losses[0]
+    rel = S.scaled_rel_error(sur.predict(theta[n:]), curves[n:])
+    assert np.median(rel) < 1.5e-3, np.median(rel)  # surrogate vs the engine it stands in for
+
+    eng = S.CurveEngine(setup, data=data)
+    sur.bind_data(data)
+    start = M.run_delayed(eng, sur, M.initial_walkers(64, S.TRUTH, seed=3), 300, seed=4, substeps=16).chain[-1]
+    plain = M.run_plain(eng, start, 200, seed=5)
+    da = M.run_delayed(eng, sur, start, 200, seed=5, substeps=16)
+    sig = plain.chain.reshape(-1, 5).std(axis=0)
+    per_eval = (_msjd(da, sig) / da.engine_evals) / (_msjd(plain, sig) / plain.engine_evals)
+    per_s = (_msjd(da, sig) / da.seconds) / (_msjd(plain, sig) / plain.seconds)
+    assert per_eval > 2.5 and per_s > 1.5, (per_eval, per_s, da.acceptance, plain.acceptance)

@@ -1,0 +1,74 @@
+"""The samplers' logic on the CPU, with a Gaussian stand-in for the engine.
+
+Delayed acceptance must leave the engine's posterior unchanged whatever the
+surrogate: here the surrogate is deliberately wrong (shifted mean, wrong
+widths), and the delayed-acceptance chains must still reproduce the target's
+mean and spread, as the plain chains do.  Tolerances: 0.15 sigma on means and
+15% on standard deviations (Monte Carlo error of ~60k correlated samples).
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def M():
+    return importlib.import_module("lcurve-rs_b200.mcmc")
+
+
+@pytest.fixture(scope="module")
+def S():
+    return importlib.import_module("lcurve-rs_b200.surrogate")
+
+
+class Gaussian:
+    """chisq of a Gaussian in the parameters (widths 2% of the prior box)."""
+
+    def __init__(self, S, mu, frac, shift=0.0):
+        self.mu = mu + shift * frac * (S.PRIOR_HI - S.PRIOR_LO)
+        self.sig = frac * (S.PRIOR_HI - S.PRIOR_LO)
+        self.evals = 0
+
+    def chisq(self, theta, scale=True):
+        theta = np.atleast_2d(theta)
+        self.evals += theta.shape[0]
+        return np.sum(((theta - self.mu) / self.sig) ** 2, axis=1)
+
+
+def _check(run, target, burn=0.3):
+    ch = run.chain[int(burn * run.chain.shape[0]):].reshape(-1, run.chain.shape[2])
+    assert np.all(np.abs(ch.mean(0) - target.mu) < 0.15 * target.sig), (ch.mean(0), target.mu)
+    assert np.all(np.abs(ch.std(0) / target.sig - 1.0) < 0.15), ch.std(0) / target.sig
+
+
+def test_plain_and_delayed_sample_the_engine_posterior(M, S):
+    mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
+    eng = Gaussian(S, mu, 0.02)
+    bad = Gaussian(S, mu, 0.03, shift=0.7)  # wrong centre and widths
+    p0 = M.initial_walkers(64, mu, seed=1, spread=0.02)
+    plain = M.run_plain(eng, p0, 1500, seed=2)
+    _check(plain, eng)
+    for k in (1, 4):
+        eng.evals = 0
+        da = M.run_delayed(eng, bad, p0, 1500, seed=3 + k, substeps=k)
+        _check(da, eng)
+        assert da.engine_evals == eng.evals <= 64 + 1500 * 64
+
+
+def test_delayed_acceptance_with_the_exact_surrogate_accepts_every_screened_move(M, S):
+    mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
+    eng = Gaussian(S, mu, 0.02)
+    p0 = M.initial_walkers(32, mu, seed=1, spread=0.02)
+    da = M.run_delayed(eng, Gaussian(S, mu, 0.02), p0, 50, seed=9, substeps=3)
+    assert da.accepted == da.stage1_pass > 0
+
+
+def test_integrated_time_of_an_ar1_chain(M):
+    rng = np.random.default_rng(0)
+    n, w, rho = 20000, 8, 0.9
+    x = np.zeros((n, w, 1))
+    for t in range(1, n):
+        x[t] = rho * x[t - 1] + rng.standard_normal((w, 1))
+    tau = M.integrated_time(x)[0]
+    assert abs(tau - (1 + rho) / (1 - rho)) < 0.1 * (1 + rho) / (1 - rho)
