@@ -18,7 +18,7 @@ data (lcurve-rs_b200/workloads.py).
           engine, the BF16 tensor-core MLP trained on them, then 256-walker
           delayed-acceptance MCMC against plain engine MCMC from one burned-in
           ensemble: ESS/s of each, surrogate error, posterior agreement.
-          Defaults are a reduced run (524k curves, 2000 steps); --mcmc-full
+          Defaults are a reduced run (524k curves, 3000 steps); --mcmc-full
           runs the full 1M-curve, 20000-step configuration.
 
 Multi-GPU (torchrun): weak scaling, each rank evaluates its own 1024-model
@@ -64,9 +64,10 @@ def parse():
                    help="full size: 1M training curves, 300 epochs, 20000 steps")
     p.add_argument("--mcmc-curves", type=int, default=524288)
     p.add_argument("--mcmc-epochs", type=int, default=250)
-    p.add_argument("--mcmc-steps", type=int, default=2000)
+    p.add_argument("--mcmc-steps", type=int, default=3000)
     p.add_argument("--mcmc-burn", type=int, default=500)
-    p.add_argument("--mcmc-substeps", type=int, default=32)
+    p.add_argument("--mcmc-substeps", type=int, default=2)
+    p.add_argument("--mcmc-bandwidth", type=float, default=0.6, help="KDE bandwidth in units of Scott's factor")
     a = p.parse_args()
     if a.mcmc_full:
         a.mcmc_curves, a.mcmc_epochs, a.mcmc_steps = 1048576, 300, 20000
@@ -206,8 +207,11 @@ def run_reference(args, rank, world):
 
 def run_mcmc(args, lcb):
     """Surrogate delayed-acceptance MCMC against plain engine MCMC: 256
-    walkers on the fixed 256-phase problem (fiducial curve + 1% noise), both
-    started from one burned-in ensemble; ESS/s over the sampling loops."""
+    walkers on the fixed 256-phase problem (fiducial curve + 1% noise), all
+    samplers started from one burned-in ensemble; ESS/s over the sampling
+    loops.  Plain samplers: the stretch move (the reference fitter's emcee
+    default) and the KDE move; the delayed-acceptance sampler screens KDE
+    moves with the surrogate (and, in --mcmc-full, stretch sub-chains too)."""
     S = importlib.import_module("lcurve-rs_b200.surrogate")
     M = importlib.import_module("lcurve-rs_b200.mcmc")
     W = importlib.import_module("lcurve-rs_b200.workloads")
@@ -227,36 +231,46 @@ def run_mcmc(args, lcb):
     eng = S.CurveEngine(setup, data=data)
     sur.bind_data(data)
     p0 = M.initial_walkers(256, S.TRUTH, seed=3)
-    burn = M.run_delayed(eng, sur, p0, args.mcmc_burn, seed=4, substeps=args.mcmc_substeps)
+    burn = M.run_delayed(eng, sur, p0, args.mcmc_burn, seed=4, substeps=32)
     start = burn.chain[-1]
-    plain = M.run_plain(eng, start, args.mcmc_steps, seed=5)
-    da = M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=args.mcmc_substeps)
-    ess_p, tau_p = M.ess(plain, burn=0.0)
-    ess_d, tau_d = M.ess(da, burn=0.0)
-    post = plain.chain[-1][:128]
-    dchi = eng.chisq(post) - sur.chisq(post)
-    sp, sd = M.posterior_summary(plain, burn=0.0), M.posterior_summary(da, burn=0.0)
-    shift = max(abs(sd[k][0] - sp[k][0]) / sp[k][1] for k in sp)
+    bw, k = args.mcmc_bandwidth, args.mcmc_substeps
+    runs = {
+        "plain_stretch": M.run_plain(eng, start, args.mcmc_steps, seed=5),
+        "plain_kde": M.run_plain(eng, start, args.mcmc_steps, seed=5, move="kde", bandwidth=bw),
+        "da_kde": M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=k, move="kde", bandwidth=bw),
+    }
+    if args.mcmc_full:
+        runs["da_stretch"] = M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=32)
+    ess = {name: M.ess(r, burn=0.0) for name, r in runs.items()}
+    rate = {name: ess[name][0] / r.seconds for name, r in runs.items()}
+    post = {name: M.posterior_summary(r, burn=0.0) for name, r in runs.items()}
+    ref = post["plain_stretch"]
+    shift = {name: max(abs(p[q][0] - ref[q][0]) / ref[q][1] for q in ref) for name, p in post.items()}
+    sample = start[:128]
+    dchi = eng.chisq(sample) - sur.chisq(sample)
+    overhead = gen_s + sur.train_seconds
     return {
-        "ess_per_s_plain": ess_p / plain.seconds, "ess_per_s_da": ess_d / da.seconds,
-        "speedup": (ess_d / da.seconds) / (ess_p / plain.seconds),
-        "ess_per_s_da_incl_training": ess_d / (da.seconds + gen_s + sur.train_seconds),
-        "ess": {"plain": ess_p, "da": ess_d}, "tau": {"plain": tau_p.tolist(), "da": tau_d.tolist()},
-        "seconds": {"plain": plain.seconds, "da": da.seconds, "curve_generation": gen_s,
+        "ess_per_s": rate,
+        "speedup_vs_plain_stretch": rate["da_kde"] / rate["plain_stretch"],
+        "speedup_vs_plain_same_move": rate["da_kde"] / rate["plain_kde"],
+        "ess_per_s_da_incl_training": ess["da_kde"][0] / (runs["da_kde"].seconds + overhead),
+        "ess": {name: e[0] for name, e in ess.items()},
+        "tau": {name: e[1].tolist() for name, e in ess.items()},
+        "seconds": {**{name: r.seconds for name, r in runs.items()}, "curve_generation": gen_s,
                     "training": sur.train_seconds, "burn_in": burn.seconds},
-        "engine_evals": {"plain": plain.engine_evals, "da": da.engine_evals},
-        "surrogate_evals_da": da.surrogate_evals,
-        "acceptance": {"plain": plain.acceptance, "da": da.acceptance},
-        "posterior": {"plain": sp, "da": sd, "max_mean_shift_in_plain_sigma": shift},
+        "engine_evals": {name: r.engine_evals for name, r in runs.items()},
+        "acceptance": {name: r.acceptance for name, r in runs.items()},
+        "posterior": post, "max_mean_shift_vs_plain_stretch_in_sigma": shift,
         "surrogate": {"network": "5 -> 4 x 512 (GELU) -> 256, BF16 tcgen05 kernels, FP32 accumulation",
                       "train_curves": n, "epochs": args.mcmc_epochs, "final_loss": losses[-1],
                       "holdout_scaled_rel_err": {"median": float(np.median(rel)),
                                                  "p99": float(np.quantile(rel, 0.99)), "max": float(rel.max())},
                       "posterior_chisq_minus_engine": {"mean": float(-dchi.mean()), "std": float(dchi.std())}},
         "config": {"walkers": 256, "steps": args.mcmc_steps, "burn_in_steps": args.mcmc_burn,
-                   "substeps": args.mcmc_substeps, "phases": setup.n_phase, "stretch_a": 2.0,
+                   "da_substeps": k, "kde_bandwidth_x_scott": bw, "phases": setup.n_phase, "stretch_a": 2.0,
                    "likelihood": "-chisq/2, chisq_batch scale=True, uniform prior box of the 1024-model batch",
-                   "data": "fiducial single_small curve at 256 phases + 1% Gaussian noise, seed 42"},
+                   "data": "fiducial single_small curve at 256 phases + 1% Gaussian noise, seed 42",
+                   "timing": "wall clock of each sampling loop (host-driven; engine and surrogate on the GPU)"},
     }
 
 

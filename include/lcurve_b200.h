@@ -132,9 +132,9 @@ int lcb_light_curve(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data,
  * giving the bytes needed (a grid element takes about 160 B, a datum about
  * 80 B, each exposure sub-division about 40 B plus 8 B per 4,096 elements).
  * The first call on a device looks up the arena's device address; make that
- * first call before any CUDA stream capture begins.  All calls on a device share the arena: this library serialises
- * them and waits for each call's GPU work before returning, since calls whose
- * GPU work overlapped would race. */
+ * first call before any CUDA stream capture begins.  All calls on a device
+ * share the arena: this library serialises them and waits for each call's GPU
+ * work before returning, since calls whose GPU work overlapped would race. */
 #define LCB_NOALLOC_ARENA_BYTES (64u * 1024u * 1024u)
 int lcb_light_curve_noalloc(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
                             int scale, int rdata, double* calc_out, lcb_result* res_out);
@@ -186,7 +186,8 @@ int  lcb_batch_results(lcb_batch* b, double* chisq_out, double* calc_out, lcb_re
 int  lcb_batch_stats(const lcb_batch* b, int64_t* out8);
 /* Eclipse-search counters of the last run: [potential evaluations, gradient
  * evaluations, line-of-sight searches, lower-bound nodes, searches proven to
- * miss by the lower bound and skipped]. */
+ * miss by the lower bound and skipped].  The line-of-sight searches are
+ * exactly the reference path's (eclipse.rs:123-197 calls). */
 int  lcb_batch_search_counts(const lcb_batch* b, int64_t* out5);
 /* Same evaluation as lcb_batch_run but issued as direct launches with CUDA
  * events between the stages (events recorded inside a graph carry no timing),

@@ -75,20 +75,26 @@ int  lcb_mlp_gemm(int mode, int64_t M, int64_t N, int64_t K, const void* a_dev, 
 int  lcb_logflux_chisq(int64_t rows, int n, const float* pred_dev, const float* mean_dev, const float* sd_dev,
                        const double* flux_dev, const double* ferr_dev, int scale, double* chisq_dev, void* cuda_stream);
 
-/* `steps` stretch moves (Goodman & Weare, scale a) of n walkers against m
- * fixed complementary walkers under the surrogate posterior alone, on the
- * network's stream with no host round trip: the first stage of delayed
- * acceptance.  y_dev (n x d) and ls_dev (n: log probability -chisq/2, finite)
- * are updated in place; rnd_dev holds steps x n x 3 numbers per move: a
- * uniform for z, a uniform for the partner, ln of a uniform for acceptance.
- * Proposals outside [lo, hi] (host arrays of d) are rejected; the network
- * input of dimension k is fadd[k] + fmul[k] * (recip[k] ? 1/x : x);
+/* `steps` Metropolis moves of n walkers against m fixed complementary
+ * walkers under the surrogate posterior alone, on the network's stream with
+ * no host round trip (the sequence is captured once as a CUDA graph and
+ * replayed): the first stage of delayed acceptance.  move 0: the stretch move
+ * (Goodman & Weare, scale a); move 1: an independence proposal from the
+ * Gaussian KDE of the complementary walkers, kernel covariance
+ * kde_chol kde_chol^T with inverse kde_prec (host d x d row-major arrays).
+ * y_dev (n x d) and ls_dev (n: log probability -chisq/2, finite) are updated
+ * in place; rnd_dev holds steps x n x R numbers, R = 3 (stretch) or 3 + d
+ * (KDE): a uniform for z (stretch) or the KDE component (KDE), a uniform for
+ * the partner (stretch), ln of a uniform for acceptance, then d standard
+ * normals (KDE).  Proposals outside [lo, hi] (host arrays of d) are rejected;
+ * the network input of dimension k is fadd[k] + fmul[k] * (recip[k] ? 1/x : x);
  * chi-squared as lcb_logflux_chisq against flux_dev / ferr_dev (n_out points). */
 int  lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y_dev, double* ls_dev,
                             const double* comp_dev, const double* rnd_dev, int steps, double a, const double* lo,
                             const double* hi, const int* recip, const float* fmul, const float* fadd,
                             const float* mean_dev, const float* sd_dev, const double* flux_dev,
-                            const double* ferr_dev, int scale);
+                            const double* ferr_dev, int scale, int move, const double* kde_chol,
+                            const double* kde_prec);
 
 #ifdef __cplusplus
 }

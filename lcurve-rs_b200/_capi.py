@@ -111,7 +111,7 @@ def load():
         "lcb_mlp_gemm": ([i, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, vp], i),
         "lcb_logflux_chisq": ([i64, i, vp, vp, vp, vp, vp, i, vp, vp], i),
         "lcb_surrogate_subchain": ([vp, i64, i64, i, vp, vp, vp, vp, i, d, dp, dp, C.POINTER(i),
-                                    C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, vp, vp, i], i),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, vp, vp, i, i, dp, dp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

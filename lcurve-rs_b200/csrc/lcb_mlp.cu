@@ -427,27 +427,90 @@ __global__ void k_logflux_chisq(int rows, int n, const float* __restrict__ pred,
 // ---------------------------------------------------------------------------
 constexpr int kMaxDim = 8;
 
+enum { MOVE_STRETCH = 0, MOVE_KDE = 1 };
+
 struct StretchArgs {
     int n, m, d, n_in;
+    int move;              // MOVE_STRETCH or MOVE_KDE
+    int rstride;           // random numbers per move: 3 (stretch) or 3 + d (KDE)
     double* y;             // n x d sub-chain positions (in/out)
     double* ls;            // n surrogate log probabilities (in/out)
     const double* comp;    // m x d complementary walkers (fixed)
-    const double* rnd;     // K x n x 3: uniform for z, uniform for the partner, log uniform for acceptance
+    const double* rnd;     // K x n x rstride: uniform (z / component), uniform (partner), log uniform, d normals (KDE)
     double* yp;            // n x d proposals
-    double* lz;            // n: (d - 1) ln z, or -inf outside the prior box
+    double* lz;            // n: log proposal-density ratio, or -inf outside the prior box
+    double* lq;            // n: KDE log density at the current positions
+    double* lqp;           // n: KDE log density at the proposals
     float* xin;            // n x n_in network inputs
     double lo[kMaxDim], hi[kMaxDim];
     float fmul[kMaxDim], fadd[kMaxDim];
     int frecip[kMaxDim];
     double a;
+    const double* kde;     // device: chol[8 x 8] then prec[8 x 8] -- KDE kernel covariance h^2 S =
+                           // chol chol^T (row-major, lower) and its inverse; a buffer, not a kernel
+                           // parameter, so one captured graph serves every half-step
 };
+
+// log of the Gaussian KDE of the complementary walkers at v (up to a constant):
+// log sum_j exp(-(v - c_j)^T prec (v - c_j) / 2), accumulated with a running maximum.
+__device__ double kde_logq(const StretchArgs& A, const double* v) {
+    double mx = -INFINITY, acc = 0.0;
+    for (int j = 0; j < A.m; ++j) {
+        double dv[kMaxDim];
+        for (int k = 0; k < A.d; ++k) dv[k] = v[k] - A.comp[(size_t)j * A.d + k];
+        double qf = 0.0;
+        for (int k = 0; k < A.d; ++k) {
+            double t = 0.0;
+            for (int l = 0; l < A.d; ++l) t += A.kde[kMaxDim * kMaxDim + k * kMaxDim + l] * dv[l];
+            qf += dv[k] * t;
+        }
+        const double e = -0.5 * qf;
+        if (e > mx) {
+            acc = acc * exp(mx - e) + 1.0;
+            mx = e;
+        } else {
+            acc += exp(e - mx);
+        }
+    }
+    return mx + log(acc);
+}
+
+__global__ void k_kde_logq(StretchArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n || A.move != MOVE_KDE) return;
+    double v[kMaxDim];
+    for (int k = 0; k < A.d; ++k) v[k] = A.y[(size_t)i * A.d + k];
+    A.lq[i] = kde_logq(A, v);
+}
 
 // Goodman & Weare stretch proposal y' = c + z (y - c), z ~ g(z) on [1/a, a];
 // the network input of y' is fadd + fmul * (y' or 1/y') per dimension.
+//
+// KDE move (emcee's KDEMove): an independence proposal from the Gaussian KDE of
+// the complementary walkers, y' = c_j + chol eps, with log density ratio
+// log q(y) - log q(y').
 __global__ void k_stretch_propose(StretchArgs A, int step) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
-    const double* r = A.rnd + ((size_t)step * A.n + i) * 3;
+    const double* r = A.rnd + ((size_t)step * A.n + i) * A.rstride;
+    if (A.move == MOVE_KDE) {
+        const int j = min((int)(r[0] * A.m), A.m - 1);
+        double v[kMaxDim];
+        bool inside = true;
+        for (int k = 0; k < A.d; ++k) {
+            double t = 0.0;
+            for (int l = 0; l <= k; ++l) t += A.kde[k * kMaxDim + l] * r[3 + l];
+            v[k] = A.comp[(size_t)j * A.d + k] + t;
+            A.yp[(size_t)i * A.d + k] = v[k];
+            inside = inside && v[k] >= A.lo[k] && v[k] <= A.hi[k];
+            const double f = A.frecip[k] ? 1.0 / v[k] : v[k];
+            A.xin[(size_t)i * A.n_in + k] = (float)__dadd_rn((double)A.fadd[k], __dmul_rn((double)A.fmul[k], f));
+        }
+        const double lqp = kde_logq(A, v);
+        A.lqp[i] = lqp;
+        A.lz[i] = inside ? A.lq[i] - lqp : -INFINITY;
+        return;
+    }
     // explicitly rounded operations (no contraction), so the moves are the
     // ones a host implementation of the same formulas makes
     double z = __dadd_rn(__dmul_rn(A.a - 1.0, r[0]), 1.0);
@@ -475,10 +538,11 @@ __global__ void k_stretch_accept(StretchArgs A, const double* __restrict__ chi, 
     if (lz == -INFINITY) return;
     double lsp = -0.5 * chi[i];
     if (!(lsp == lsp)) lsp = -INFINITY;
-    const double logu = A.rnd[((size_t)step * A.n + i) * 3 + 2];
+    const double logu = A.rnd[((size_t)step * A.n + i) * A.rstride + 2];
     if (logu < lz + lsp - A.ls[i]) {
         for (int k = 0; k < A.d; ++k) A.y[(size_t)i * A.d + k] = A.yp[(size_t)i * A.d + k];
         A.ls[i] = lsp;
+        if (A.move == MOVE_KDE) A.lq[i] = A.lqp[i];
     }
 }
 
@@ -552,6 +616,15 @@ void launch_gemm_mode(const CUtensorMap& ta, const CUtensorMap& tb, const GemmAr
     CK(cudaGetLastError());
 }
 
+// Sets the dynamic shared-memory limit of every GEMM variant (needed before a
+// stream capture, during which the first launch of a variant cannot set it).
+void prepare_gemm_attributes() {
+    CK(cudaFuncSetAttribute(k_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    CK(cudaFuncSetAttribute(k_gemm<EPI_BIAS_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    CK(cudaFuncSetAttribute(k_gemm<EPI_BIAS_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    CK(cudaFuncSetAttribute(k_gemm<EPI_DGELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+}
+
 void gemm(int mode, int64_t M, int64_t N, int64_t K, const void* A, const void* B, const float* bias, const float* aux,
           void* out, void* out2, int* err, cudaStream_t s) {
     if (M <= 0 || N <= 0 || K <= 0 || N % 8 || K % 8 || M > INT32_MAX || N > 65535 * (int64_t)BN)
@@ -615,7 +688,12 @@ struct lcb_mlp {
     DBuf<int> err;
     DBuf<double> loss;
     DBuf<float> sub_x;                   // sub-chain: network inputs
-    DBuf<double> sub_yp, sub_lz, sub_chi;  // proposals, (d-1) ln z, chi-squared
+    DBuf<double> sub_yp, sub_lz, sub_chi;  // proposals, log proposal ratio, chi-squared
+    DBuf<double> sub_lq, sub_lqp;          // KDE log densities (current, proposed)
+    DBuf<double> sub_kde;                  // KDE factors of the current call
+    DBuf<double> sub_y, sub_ls, sub_comp, sub_rnd;  // fixed copies of the sub-chain's inputs (graph operands)
+    cudaGraphExec_t sub_graph = nullptr;   // the captured K-step sub-chain
+    std::vector<unsigned char> sub_key;    // what the captured graph depends on
     int64_t steps = 0;
 
     const float* W(int l) const { return p.p + tab.off[l]; }
@@ -628,7 +706,10 @@ struct lcb_mlp {
         if (stream) cudaStreamSynchronize(stream);
         p.free(); m.free(); v.free(); g.free(); wbf.free(); wtbf.free(); x0.free(); pred.free(); dzt.free(); xt.free();
         dz[0].free(); dz[1].free(); err.free(); loss.free();
-        sub_x.free(); sub_yp.free(); sub_lz.free(); sub_chi.free();
+        sub_x.free(); sub_yp.free(); sub_lz.free(); sub_chi.free(); sub_lq.free(); sub_lqp.free(); sub_kde.free();
+        sub_y.free(); sub_ls.free(); sub_comp.free(); sub_rnd.free();
+        if (sub_graph) cudaGraphExecDestroy(sub_graph);
+        sub_graph = nullptr;
         for (auto& t : y) t.free();
         for (auto& t : z) t.free();
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -762,6 +843,12 @@ int lcb_mlp_create(int device, int n_in, int width, int n_hidden, int n_out, int
         N->sub_yp.alloc(B * kMaxDim);
         N->sub_lz.alloc(B);
         N->sub_chi.alloc(B);
+        N->sub_lq.alloc(B);
+        N->sub_lqp.alloc(B);
+        N->sub_kde.alloc(2 * kMaxDim * kMaxDim);
+        N->sub_y.alloc(B * kMaxDim);
+        N->sub_ls.alloc(B);
+        N->sub_comp.alloc(B * kMaxDim);
         // He-uniform initial weights, zero biases (padding columns stay zero)
         std::vector<float> h(off, 0.f);
         std::mt19937_64 rng(seed);
@@ -921,34 +1008,102 @@ int lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y_
                            const double* comp_dev, const double* rnd_dev, int steps, double a, const double* lo,
                            const double* hi, const int* recip, const float* fmul, const float* fadd,
                            const float* mean_dev, const float* sd_dev, const double* flux_dev, const double* ferr_dev,
-                           int scale) {
+                           int scale, int move, const double* kde_chol, const double* kde_prec) {
     if (!net || !y_dev || !ls_dev || !comp_dev || !rnd_dev || !lo || !hi || !recip || !fmul || !fadd || !mean_dev ||
-        !sd_dev || !flux_dev || !ferr_dev)
+        !sd_dev || !flux_dev || !ferr_dev || (move == MOVE_KDE && (!kde_chol || !kde_prec)))
         return LCB_ERR_INVALID;
     return guard([&] {
         if (n <= 0 || n > net->max_batch || m <= 0 || m > INT32_MAX || d != net->n_in || d > kMaxDim || steps < 0 ||
             !(a > 1.0))
             throw Fail(LCB_ERR_INVALID, "sub-chain: 0 < n <= max_batch, d == n_in <= 8, a > 1 required");
+        if (move != MOVE_STRETCH && move != MOVE_KDE) throw Fail(LCB_ERR_INVALID, "sub-chain: unknown move");
+        if (m > net->max_batch) throw Fail(LCB_ERR_INVALID, "sub-chain: at most max_batch complementary walkers");
         CK(cudaSetDevice(net->device));
+        if (steps == 0) return;
+        cudaStream_t st = net->stream;
+        const int rstride = move == MOVE_KDE ? 3 + d : 3;
+        const size_t nrnd = (size_t)steps * n * rstride;
+        if (net->sub_rnd.n < nrnd) {  // grow the random-number buffer (outside any capture)
+            CK(cudaStreamSynchronize(st));
+            net->sub_rnd.free();
+            net->sub_rnd.alloc(nrnd);
+            if (net->sub_graph) cudaGraphExecDestroy(net->sub_graph);
+            net->sub_graph = nullptr;
+        }
         StretchArgs A{};
         A.n = (int)n; A.m = (int)m; A.d = d; A.n_in = net->n_in;  // rows of lcb_mlp_forward input: n_in wide
-        A.y = y_dev; A.ls = ls_dev; A.comp = comp_dev; A.rnd = rnd_dev;
+        A.y = net->sub_y.p; A.ls = net->sub_ls.p; A.comp = net->sub_comp.p; A.rnd = net->sub_rnd.p;
         A.yp = net->sub_yp.p; A.lz = net->sub_lz.p; A.xin = net->sub_x.p;
+        A.lq = net->sub_lq.p; A.lqp = net->sub_lqp.p;
+        A.move = move; A.rstride = rstride;
+        double kde[2 * kMaxDim * kMaxDim] = {};
         for (int k = 0; k < d; ++k) {
             A.lo[k] = lo[k]; A.hi[k] = hi[k]; A.frecip[k] = recip[k]; A.fmul[k] = fmul[k]; A.fadd[k] = fadd[k];
+            if (move == MOVE_KDE)
+                for (int l = 0; l < d; ++l) {
+                    kde[k * kMaxDim + l] = l <= k ? kde_chol[k * d + l] : 0.0;
+                    kde[kMaxDim * kMaxDim + k * kMaxDim + l] = kde_prec[k * d + l];
+                }
         }
+        A.kde = net->sub_kde.p;
         A.a = a;
-        const unsigned g = (unsigned)((n + 127) / 128);
-        for (int k = 0; k < steps; ++k) {
-            k_stretch_propose<<<g, 128, 0, net->stream>>>(A, k);
-            CK(cudaGetLastError());
-            net->forward(net->sub_x.p, n, nullptr);
-            k_logflux_chisq<<<(unsigned)n, 128, 0, net->stream>>>((int)n, net->n_out, net->pred.p, mean_dev, sd_dev,
-                                                                 flux_dev, ferr_dev, scale, net->sub_chi.p);
-            CK(cudaGetLastError());
-            k_stretch_accept<<<g, 128, 0, net->stream>>>(A, net->sub_chi.p, k);
-            CK(cudaGetLastError());
+        // the graph is valid while everything it was captured with is unchanged
+        std::vector<unsigned char> key(sizeof(A) + 6 * sizeof(int64_t) + 4 * sizeof(void*));
+        {
+            unsigned char* q = key.data();
+            auto put = [&](const void* v, size_t b) { std::memcpy(q, v, b); q += b; };
+            put(&A, sizeof(A));
+            const int64_t ints[6] = {n, m, d, steps, scale, (int64_t)net->sub_rnd.n};
+            put(ints, sizeof(ints));
+            const void* ptrs[4] = {mean_dev, sd_dev, flux_dev, ferr_dev};
+            put(ptrs, sizeof(ptrs));
         }
+        CK(cudaMemcpyAsync(net->sub_y.p, y_dev, n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(net->sub_ls.p, ls_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(net->sub_comp.p, comp_dev, m * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(net->sub_rnd.p, rnd_dev, nrnd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (move == MOVE_KDE) {  // pageable source: the copy is staged before this call returns
+            CK(cudaMemcpyAsync(net->sub_kde.p, kde, sizeof(kde), cudaMemcpyHostToDevice, st));
+        }
+        auto enqueue = [&] {
+            const unsigned g = (unsigned)((n + 127) / 128);
+            if (move == MOVE_KDE) {
+                k_kde_logq<<<g, 128, 0, st>>>(A);
+                CK(cudaGetLastError());
+            }
+            for (int k = 0; k < steps; ++k) {
+                k_stretch_propose<<<g, 128, 0, st>>>(A, k);
+                CK(cudaGetLastError());
+                net->forward(net->sub_x.p, n, nullptr);
+                k_logflux_chisq<<<(unsigned)n, 128, 0, st>>>((int)n, net->n_out, net->pred.p, mean_dev, sd_dev,
+                                                            flux_dev, ferr_dev, scale, net->sub_chi.p);
+                CK(cudaGetLastError());
+                k_stretch_accept<<<g, 128, 0, st>>>(A, net->sub_chi.p, k);
+                CK(cudaGetLastError());
+            }
+        };
+        if (!net->sub_graph || net->sub_key != key) {
+            if (net->sub_graph) cudaGraphExecDestroy(net->sub_graph);
+            net->sub_graph = nullptr;
+            net->sub_key.clear();
+            prepare_gemm_attributes();  // function attributes are set outside the capture
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue();
+            } catch (...) {
+                if (cudaStreamEndCapture(st, &graph) == cudaSuccess && graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            CK(cudaStreamEndCapture(st, &graph));
+            cudaError_t e = cudaGraphInstantiate(&net->sub_graph, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(e);
+            net->sub_key = key;
+        }
+        CK(cudaGraphLaunch(net->sub_graph, st));
+        CK(cudaMemcpyAsync(y_dev, net->sub_y.p, n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ls_dev, net->sub_ls.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     });
 }
 

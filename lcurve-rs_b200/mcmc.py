@@ -22,7 +22,10 @@ walker whose sub-chain moved it from x to y is then judged by the engine,
   stage 2  accept y with min(1, exp(l(y) - l(x) - l~(y) + l~(x)))
            l = engine log probability,
 
-else it stays at x.  With substeps = 1 this is Christen & Fox's two-stage
+else it stays at x.  Moves are the stretch move or, as emcee's KDEMove, an
+independence proposal from a Gaussian KDE of the other half (valid because
+that half is held fixed); the plain sampler offers the same two moves.
+With substeps = 1 this is Christen & Fox's two-stage
 delayed acceptance; with more sub-steps it is the surrogate transition method
 (Liu 2001, sec. 9.4.3).  Either way the pair of stages satisfies detailed
 balance with respect to the engine's posterior, so both samplers target the
@@ -58,30 +61,79 @@ def _stretch(rng, xs, xc, a):
     return xc[j] + z[:, None] * (xs - xc[j]), z
 
 
-def subchain_numbers(rng, steps: int, n: int) -> np.ndarray:
-    """steps x n x 3 random numbers of a surrogate sub-chain: a uniform for the
-    stretch factor, a uniform for the partner, ln of a uniform for acceptance."""
+@dataclasses.dataclass
+class KDE:
+    """Gaussian KDE of the complementary walkers (emcee's KDEMove): kernel
+    covariance h^2 S with S their sample covariance and h Scott's factor
+    m^(-1/(d+4)).  Proposals from it are independent of the moving walker,
+    which is what keeps the move valid with the complement held fixed."""
+
+    comp: np.ndarray
+    chol: np.ndarray
+    prec: np.ndarray
+
+    @classmethod
+    def of(cls, comp: np.ndarray, bandwidth: float = 1.0) -> "KDE":
+        """bandwidth multiplies Scott's factor (1 = emcee's default)."""
+        m, d = comp.shape
+        h2 = (bandwidth * m ** (-1.0 / (d + 4))) ** 2
+        cov = np.cov(comp, rowvar=False) * h2
+        cov = cov + np.diag(1e-12 * np.diag(cov) + 1e-300)
+        return cls(comp, np.linalg.cholesky(cov), np.linalg.inv(cov))
+
+    def logq(self, y: np.ndarray) -> np.ndarray:
+        diff = y[:, None, :] - self.comp[None, :, :]
+        e = -0.5 * np.einsum("nmi,ij,nmj->nm", diff, self.prec, diff)
+        mx = e.max(axis=1, keepdims=True)
+        return mx[:, 0] + np.log(np.exp(e - mx).sum(axis=1))
+
+    def draw(self, r: np.ndarray) -> np.ndarray:
+        """Proposals for one move: r[:, 0] picks the component, r[:, 3:] are normals."""
+        m = self.comp.shape[0]
+        j = np.minimum((r[:, 0] * m).astype(np.int64), m - 1)
+        return self.comp[j] + r[:, 3:] @ self.chol.T
+
+
+MOVES = ("stretch", "kde")
+
+
+def subchain_numbers(rng, steps: int, n: int, move: str = "stretch", d: int = 5) -> np.ndarray:
+    """steps x n x R random numbers of a surrogate sub-chain: a uniform for the
+    stretch factor (or the KDE component), a uniform for the partner, ln of a
+    uniform for acceptance, and for the KDE move d standard normals."""
     r = rng.random((steps, n, 3))
     with np.errstate(divide="ignore"):
         r[..., 2] = np.log(r[..., 2])
+    if move == "kde":
+        r = np.concatenate([r, rng.standard_normal((steps, n, d))], axis=2)
     return r
 
 
-def subchain_host(surrogate, y, ls, comp, rnd, a=2.0):
+def subchain_host(surrogate, y, ls, comp, rnd, a=2.0, move="stretch", bandwidth=1.0):
     """The surrogate sub-chain on the host, one surrogate call per move; the
     same arithmetic as the device sub-chain (lcb_surrogate_subchain)."""
     y, ls = y.copy(), ls.copy()
     n, d = y.shape
     m = comp.shape[0]
+    kde = KDE.of(comp, bandwidth) if move == "kde" else None
+    lq = kde.logq(y) if kde else None
     for r in rnd:
-        z = ((a - 1.0) * r[:, 0] + 1.0) ** 2 / a
-        j = np.minimum((r[:, 1] * m).astype(np.int64), m - 1)
-        yp = comp[j] + z[:, None] * (y - comp[j])
+        if kde:
+            yp = kde.draw(r)
+            lqp = kde.logq(yp)
+            lratio = lq - lqp
+        else:
+            z = ((a - 1.0) * r[:, 0] + 1.0) ** 2 / a
+            j = np.minimum((r[:, 1] * m).astype(np.int64), m - 1)
+            yp = comp[j] + z[:, None] * (y - comp[j])
+            lratio = (d - 1) * np.log(z)
         prior = log_prior(yp)
         lsp = prior + _loglike(surrogate.chisq(yp, scale=True))
-        take = np.isfinite(prior) & (r[:, 2] < (d - 1) * np.log(z) + lsp - ls)
+        take = np.isfinite(prior) & (r[:, 2] < lratio + lsp - ls)
         y[take] = yp[take]
         ls[take] = lsp[take]
+        if kde:
+            lq[take] = lqp[take]
     return y, ls
 
 
@@ -116,7 +168,8 @@ def _eval_prob(engine, theta):
     return out
 
 
-def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0) -> Run:
+def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0, move: str = "stretch",
+              bandwidth: float = 1.0) -> Run:
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -130,9 +183,15 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
         perm = rng.permutation(nw)
         for h in (0, 1):
             S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
-            y, z = _stretch(rng, x[S], x[Cc], a)
+            if move == "kde":
+                kde = KDE.of(x[Cc], bandwidth)
+                y = kde.draw(subchain_numbers(rng, 1, len(S), "kde", d)[0])
+                lratio = kde.logq(x[S]) - kde.logq(y)
+            else:
+                y, z = _stretch(rng, x[S], x[Cc], a)
+                lratio = (d - 1) * np.log(z)
             lpy = _eval_prob(engine, y)
-            loga = (d - 1) * np.log(z) + lpy - lp[S]
+            loga = lratio + lpy - lp[S]
             take = np.log(rng.random(len(S))) < loga
             x[S[take]] = y[take]
             lp[S[take]] = lpy[take]
@@ -143,7 +202,8 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
 
 
 def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0,
-                substeps: int = 1, device_subchain: bool | None = None) -> Run:
+                substeps: int = 1, device_subchain: bool | None = None, move: str = "stretch",
+                bandwidth: float = 1.0) -> Run:
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -160,11 +220,11 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
         for h in (0, 1):
             S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
             # stage 1: a surrogate sub-chain for every walker of the half
-            rnd = subchain_numbers(rng, substeps, len(S))
+            rnd = subchain_numbers(rng, substeps, len(S), move, d)
             if on_device:
-                y, lsy = surrogate.subchain(x[S], lps[S], x[Cc], rnd, a)
+                y, lsy = surrogate.subchain(x[S], lps[S], x[Cc], rnd, a, move=move, bandwidth=bandwidth)
             else:
-                y, lsy = subchain_host(surrogate, x[S], lps[S], x[Cc], rnd, a)
+                y, lsy = subchain_host(surrogate, x[S], lps[S], x[Cc], rnd, a, move=move, bandwidth=bandwidth)
             nsur += substeps * len(S)
             moved = np.any(y != x[S], axis=1)
             # stage 2: the engine judges the walkers that moved

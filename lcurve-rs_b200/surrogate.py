@@ -295,13 +295,22 @@ class Surrogate:
         return out
 
     def subchain(self, y: np.ndarray, ls: np.ndarray, comp: np.ndarray, rnd: np.ndarray, a: float = 2.0,
-                 scale: bool = True):
-        """Runs rnd.shape[0] surrogate stretch moves of the walkers y (log
-        probabilities ls) against the fixed walkers comp on the device
-        (lcb_surrogate_subchain); returns the new (y, ls)."""
+                 scale: bool = True, move: str = "stretch", bandwidth: float = 1.0):
+        """Runs rnd.shape[0] surrogate Metropolis moves (stretch or KDE) of the
+        walkers y (log probabilities ls) against the fixed walkers comp on the
+        device (lcb_surrogate_subchain); returns the new (y, ls)."""
         torch = _torch()
+        from .mcmc import KDE  # noqa: PLC0415
         y = np.ascontiguousarray(y, dtype=np.float64)
         n, d = y.shape
+        if move == "kde":
+            kde = KDE.of(np.asarray(comp, dtype=np.float64), bandwidth)
+            keep = (np.ascontiguousarray(kde.chol), np.ascontiguousarray(kde.prec))  # alive through the call
+            chol = keep[0].ctypes.data_as(C.POINTER(C.c_double))
+            prec = keep[1].ctypes.data_as(C.POINTER(C.c_double))
+        else:
+            chol = prec = None
+            keep = ()
         with torch.cuda.stream(self._stream):
             yd = torch.as_tensor(y).to(self.dev)
             lsd = torch.as_tensor(np.ascontiguousarray(ls, dtype=np.float64)).to(self.dev)
@@ -312,5 +321,6 @@ class Surrogate:
                 C.c_void_p(cd.data_ptr()), C.c_void_p(rd.data_ptr()), rnd.shape[0], a, self._c_lo, self._c_hi,
                 self._c_recip, self._c_fmul, self._c_fadd, C.c_void_p(self.mean.data_ptr()),
                 C.c_void_p(self.sd.data_ptr()), C.c_void_p(self._flux.data_ptr()), C.c_void_p(self._ferr.data_ptr()),
-                int(bool(scale))))
+                int(bool(scale)), 1 if move == "kde" else 0, chol, prec))
+            del keep
             return yd.cpu().numpy(), lsd.cpu().numpy()

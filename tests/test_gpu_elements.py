@@ -68,7 +68,7 @@ def test_grids_match_oracle(lcb, oracle, W, case):
     assert total > 0
 
 
-def test_roche_search_counts_and_skips(lcb, W):
+def test_roche_search_counts_and_skips(lcb, oracle, W):
     specs = W.batch_models(n=4, seed=9, nlat1=(30, 40), nlat2=(30, 40), ntime=(50, 60))
     models = [lcb.Model(text=s) for s, _ in specs]
     offs = np.cumsum([0] + [len(t) for _, t in specs])
@@ -78,3 +78,10 @@ def test_roche_search_counts_and_skips(lcb, W):
     c = B.search_counts()
     assert c["searches"] > 0 and c["proven_misses"] > 0
     assert c["proven_misses"] <= c["searches"]
+    # the device makes exactly the reference path's line-of-sight searches (a proven
+    # miss replaces a search's evaluations, not its decision)
+    oracle.counters_reset()
+    for (text, t), lo, hi in zip(specs, offs[:-1], offs[1:]):
+        oracle.Model(text=text).light_curve(data[lo:hi], nthreads=1)
+    ref = oracle.counters()["fblink"]
+    assert c["searches"] == ref, (c, ref)

@@ -36,7 +36,8 @@ def _problem(S, W):
     return setup, data
 
 
-def test_device_subchain_matches_host_loop(lcb, mods):
+@pytest.mark.parametrize("move", ["stretch", "kde"])
+def test_device_subchain_matches_host_loop(lcb, mods, move):
     S, M, W = mods
     setup, data = _problem(S, W)
     sur = S.Surrogate(seed=2)  # untrained weights are enough to compare the two paths
@@ -45,9 +46,9 @@ def test_device_subchain_matches_host_loop(lcb, mods):
     walkers = M.initial_walkers(128, S.TRUTH, seed=1, spread=0.05)
     y, comp = walkers[:64], walkers[64:]
     ls = -0.5 * sur.chisq(y)
-    rnd = M.subchain_numbers(rng, 6, 64)
-    yd, lsd = sur.subchain(y, ls, comp, rnd)
-    yh, lsh = M.subchain_host(sur, y, ls, comp, rnd)
+    rnd = M.subchain_numbers(rng, 6, 64, move)
+    yd, lsd = sur.subchain(y, ls, comp, rnd, move=move)
+    yh, lsh = M.subchain_host(sur, y, ls, comp, rnd, move=move)
     same = np.all(np.isclose(yd, yh, rtol=1e-12, atol=0), axis=1)
     # identical moves except where float rounding of the network input decides a tie
     assert same.mean() >= 0.95
@@ -70,10 +71,11 @@ def test_trained_surrogate_gains_over_plain_mcmc(lcb, mods):
 
     eng = S.CurveEngine(setup, data=data)
     sur.bind_data(data)
-    start = M.run_delayed(eng, sur, M.initial_walkers(64, S.TRUTH, seed=3), 300, seed=4, substeps=16).chain[-1]
-    plain = M.run_plain(eng, start, 200, seed=5)
-    da = M.run_delayed(eng, sur, start, 200, seed=5, substeps=16)
+    start = M.run_delayed(eng, sur, M.initial_walkers(256, S.TRUTH, seed=3), 300, seed=4, substeps=32).chain[-1]
+    # same move (KDE proposals from the other half) with and without the surrogate screen, 256 walkers
+    plain = M.run_plain(eng, start, 200, seed=5, move="kde", bandwidth=0.6)
+    da = M.run_delayed(eng, sur, start, 200, seed=5, substeps=2, move="kde", bandwidth=0.6)
     sig = plain.chain.reshape(-1, 5).std(axis=0)
     per_eval = (_msjd(da, sig) / da.engine_evals) / (_msjd(plain, sig) / plain.engine_evals)
     per_s = (_msjd(da, sig) / da.seconds) / (_msjd(plain, sig) / plain.seconds)
-    assert per_eval > 2.5 and per_s > 1.5, (per_eval, per_s, da.acceptance, plain.acceptance)
+    assert per_eval > 3.0 and per_s > 1.5, (per_eval, per_s, da.acceptance, plain.acceptance)

@@ -56,6 +56,31 @@ def test_plain_and_delayed_sample_the_engine_posterior(M, S):
         assert da.engine_evals == eng.evals <= 64 + 1500 * 64
 
 
+def test_kde_moves_sample_the_engine_posterior(M, S):
+    mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
+    eng = Gaussian(S, mu, 0.02)
+    bad = Gaussian(S, mu, 0.03, shift=0.7)
+    p0 = M.initial_walkers(64, mu, seed=1, spread=0.02)
+    _check(M.run_plain(eng, p0, 600, seed=2, move="kde"), eng)
+    _check(M.run_delayed(eng, bad, p0, 600, seed=3, substeps=4, move="kde"), eng)
+
+
+def test_kde_density_and_draws(M):
+    rng = np.random.default_rng(0)
+    comp = rng.normal(size=(200, 5)) * np.array([1.0, 2.0, 0.5, 3.0, 1.0])
+    kde = M.KDE.of(comp)
+    r = M.subchain_numbers(rng, 1, 20000, "kde", 5)[0]
+    y = kde.draw(r)
+    # the KDE's covariance is S (1 + h^2): draws spread slightly wider than the walkers
+    h2 = 200 ** (-2.0 / 9)
+    assert np.allclose(y.std(0), comp.std(0, ddof=1) * np.sqrt(1 + h2), rtol=0.05)
+    # logq is the log of the mixture density up to one constant
+    lq = kde.logq(y[:5])
+    diff = y[:5, None, :] - comp[None]
+    dens = np.exp(-0.5 * np.einsum("nmi,ij,nmj->nm", diff, kde.prec, diff)).sum(1)
+    assert np.allclose(lq, np.log(dens))
+
+
 def test_delayed_acceptance_with_the_exact_surrogate_accepts_every_screened_move(M, S):
     mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
     eng = Gaussian(S, mu, 0.02)
