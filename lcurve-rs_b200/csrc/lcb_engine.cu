@@ -86,6 +86,8 @@ struct lcb_ctx {
     std::mutex mu;
     std::string last_error;
     DeviceSet scratch;  // buffers of transient (non-resident) calls
+    lcb::Plan plan;     // plan of the last transient call (its buffers are reused)
+    std::vector<lcb_datum> stage;  // host staging of gathered data
     cudaEvent_t ev[kStages + 1] = {};
     int64_t h2d = 0, d2h = 0;  // bytes moved by the current / last call
 };
@@ -130,11 +132,18 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     put(D.dmodel, P.datum_model.data(), P.datum_model.size() * sizeof(int32_t));
     put(D.dsub0, P.datum_sub0.data(), P.datum_sub0.size() * sizeof(int64_t));
     if (upload_data) {
-        // expanded (model, datum) records; shared data is gathered on the host once
-        std::vector<lcb_datum> ex(P.ndatum);
-        for (int64_t d = 0; d < P.ndatum; ++d) ex[d] = data[P.datum_src[d]];
         (void)ndata_src;
-        put(D.datum, ex.data(), ex.size() * sizeof(lcb_datum));
+        if (P.datum_contiguous && P.ndatum > 0) {
+            // ragged data laid out model after model: one copy straight from the caller's buffer
+            put(D.datum, data + P.datum_src[0], P.ndatum * sizeof(lcb_datum));
+        } else {
+            // expanded (model, datum) records; shared data is gathered on the host once
+            std::vector<lcb_datum>& ex = C->stage;
+            ex.resize(P.ndatum);
+            for (int64_t d = 0; d < P.ndatum; ++d) ex[d] = data[P.datum_src[d]];
+            put(D.datum, ex.data(), ex.size() * sizeof(lcb_datum));
+            // the copy is from pageable memory: it is staged before cudaMemcpyAsync returns
+        }
     }
     D.rec.ensure(P.nelem * sizeof(float4));
     D.pos.ensure(P.nelem * sizeof(float4));
@@ -512,7 +521,7 @@ int lcb_chisq_batch(lcb_ctx* C, const lcb_model* base, const lcb_datum* data, in
         std::vector<int64_t> st(nsets, 0), cnt(nsets, n);
         std::vector<double> res;
         std::vector<int> status;
-        lcb::Plan P;
+        lcb::Plan& P = C->plan;
         run_transient(C, mp.data(), nsets, data, st.data(), cnt.data(), scale, 1, res, nullptr, P, status);
         for (int64_t i = 0; i < nsets; ++i) chisq_out[i] = P.model_ok[i] ? res[i * 12 + 1] : NAN;
     });
@@ -535,7 +544,7 @@ int lcb_chisq_batch_ragged(lcb_ctx* C, const lcb_model* const* models, int64_t n
         }
         std::vector<double> res, calc;
         std::vector<int> status;
-        lcb::Plan P;
+        lcb::Plan& P = C->plan;
         run_transient(C, mp.data(), nmodels, data, st.data(), cnt.data(), scale, 1, res, calc_out ? &calc : nullptr, P,
                       status);
         for (int64_t i = 0; i < nmodels; ++i) {

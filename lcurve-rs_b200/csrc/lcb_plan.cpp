@@ -696,9 +696,27 @@ int64_t host_numface(int nlat) {
     return star_bands(m, true, nlat, false, 0, 0, 0, 0, b);
 }
 
+// Runs f(0..n) on the host's cores (items of `grain` or more per thread).
+template <class F>
+void parallel_for(int64_t n, int64_t grain, F&& f) {
+    const int64_t nthreads =
+        std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), (n + grain - 1) / std::max<int64_t>(grain, 1));
+    if (nthreads <= 1) {
+        for (int64_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::vector<std::thread> pool;
+    for (int64_t t = 0; t < nthreads; ++t)
+        pool.emplace_back([&] {
+            for (int64_t i; (i = next.fetch_add(1)) < n;) f(i);
+        });
+    for (auto& t : pool) t.join();
+}
+
 void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, const int64_t* start,
                 const int64_t* count, int num_sms, Plan& P) {
-    P = Plan();
+    P.reset();
     P.models.resize(n);
     P.model_ok.assign(n, 0);
     P.model_err.assign(n, std::string());
@@ -717,41 +735,44 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         }
     };
     // models are independent: prepare them on the host's cores (8 or more per thread)
-    const int64_t nthreads = std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), (n + 7) / 8);
-    if (nthreads <= 1) {
-        for (int64_t i = 0; i < n; ++i) prep(i);
-    } else {
-        std::atomic<int64_t> next{0};
-        std::vector<std::thread> pool;
-        for (int64_t t = 0; t < nthreads; ++t)
-            pool.emplace_back([&] {
-                for (int64_t i; (i = next.fetch_add(1)) < n;) prep(i);
-            });
-        for (auto& t : pool) t.join();
+    parallel_for(n, 8, prep);
+    // sub-phases and data: per-model sums, prefix offsets, then the per-datum
+    // arrays of each model filled in parallel
+    std::vector<int64_t> dbeg(n + 1, 0), sbeg(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) dbeg[i + 1] = dbeg[i] + std::max<int64_t>(count[i], 0);
+    P.ndatum = dbeg[n];
+    parallel_for(n, 16, [&](int64_t i) {
+        int64_t ns = 0;
+        if (P.model_ok[i])
+            for (int64_t k = 0; k < dbeg[i + 1] - dbeg[i]; ++k) ns += std::max(data[start[i] + k].ndiv, 0);
+        sbeg[i + 1] = ns;
+    });
+    for (int64_t i = 0; i < n; ++i) {
+        if (sbeg[i + 1] > INT32_MAX / 2) throw Error(LCB_ERR_INVALID, "too many sub-phases in one model");
+        sbeg[i + 1] += sbeg[i];
     }
-    // sub-phases and data
-    P.ndatum = 0;
-    for (int64_t i = 0; i < n; ++i) P.ndatum += std::max<int64_t>(count[i], 0);
     P.datum_model.resize(P.ndatum);
     P.datum_sub0.resize(P.ndatum);
     P.datum_src.resize(P.ndatum);
-    int64_t sub = 0, dd = 0;
-    for (int64_t i = 0; i < n; ++i) {
+    parallel_for(n, 16, [&](int64_t i) {
         ModelDev& D = lay[i].dev;
-        D.datum_begin = dd;
-        D.ndatum = std::max<int64_t>(count[i], 0);
-        D.sub_begin = sub;
-        for (int64_t k = 0; k < D.ndatum; ++k, ++dd) {
-            int64_t src = start[i] + k;
+        D.datum_begin = dbeg[i];
+        D.ndatum = dbeg[i + 1] - dbeg[i];
+        D.sub_begin = sbeg[i];
+        D.nsub = sbeg[i + 1] - sbeg[i];
+        int64_t sub = sbeg[i];
+        for (int64_t k = 0, dd = dbeg[i]; k < D.ndatum; ++k, ++dd) {
+            const int64_t src = start[i] + k;
             P.datum_model[dd] = (int32_t)i;
             P.datum_sub0[dd] = sub;
             P.datum_src[dd] = src;
             if (P.model_ok[i]) sub += std::max(data[src].ndiv, 0);
         }
-        D.nsub = sub - D.sub_begin;
-        if (D.nsub > INT32_MAX / 2) throw Error(LCB_ERR_INVALID, "too many sub-phases in one model");
-    }
-    P.nsub = sub;
+    });
+    P.nsub = sbeg[n];
+    P.datum_contiguous = true;
+    for (int64_t i = 1; i < n && P.datum_contiguous; ++i)
+        P.datum_contiguous = start[i] == start[i - 1] + std::max<int64_t>(count[i - 1], 0);
 
     // global element / table layout (a model's segments are contiguous)
     std::vector<size_t> seg_begin(n + 1);
@@ -773,25 +794,47 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     seg_begin[n] = P.segs.size();
     if (P.nelem > ((int64_t)1 << 34)) throw Error(LCB_ERR_INVALID, "batch too large (elements)");
 
-    // element-kernel blocks; Roche ray-march blocks (one per eclipsing Roche star); star-grid aux blocks
-    for (size_t s = 0; s < P.segs.size(); ++s) {
-        const SegDesc& g = P.segs[s];
+    // element-kernel blocks; Roche ray-march blocks (one per eclipsing Roche star); star-grid aux blocks:
+    // counts per segment, prefix offsets, then each segment's blocks written in parallel
+    const int64_t nseg = (int64_t)P.segs.size();
+    auto roche_by = [&](const SegDesc& g, int by) {
         const ModelDev& D = lay[g.model].dev;
-        for (int64_t off = 0; off < g.count; off += kElemThreads) P.eblocks.push_back(ElemBlock{(int32_t)s, 0, off});
-        bool star = g.kind == SEG_STAR1 || g.kind == SEG_STAR2;
-        if (star)
-            for (int64_t off = 0; off < g.count; off += kElemThreads) P.ablocks.push_back(ElemBlock{(int32_t)s, 0, off});
-        for (int by = 1; by <= 2; ++by) {
-            bool roche = by == 1 ? D.roche1 : D.roche2;
-            bool ecl;
-            if (g.kind == SEG_STAR1) ecl = by == 2 && D.eclipse1;
-            else if (g.kind == SEG_STAR2) ecl = by == 1 && D.eclipse2;
-            else ecl = by == 1 ? D.eclipse1 : D.eclipse2;
-            if (!(roche && ecl)) continue;
-            P.roche_elems += g.count;
-            for (int64_t off = 0; off < g.count; off += kRocheBlock) P.rblocks.push_back(ElemBlock{(int32_t)s, by, off});
-        }
+        bool roche = by == 1 ? D.roche1 : D.roche2;
+        bool ecl;
+        if (g.kind == SEG_STAR1) ecl = by == 2 && D.eclipse1;
+        else if (g.kind == SEG_STAR2) ecl = by == 1 && D.eclipse2;
+        else ecl = by == 1 ? D.eclipse1 : D.eclipse2;
+        return roche && ecl;
+    };
+    std::vector<int64_t> eb(nseg + 1, 0), ab(nseg + 1, 0), rb(nseg + 1, 0);
+    for (int64_t s = 0; s < nseg; ++s) {
+        const SegDesc& g = P.segs[s];
+        const int64_t ne = (g.count + kElemThreads - 1) / kElemThreads;
+        eb[s + 1] = eb[s] + ne;
+        ab[s + 1] = ab[s] + ((g.kind == SEG_STAR1 || g.kind == SEG_STAR2) ? ne : 0);
+        int64_t nr = 0;
+        for (int by = 1; by <= 2; ++by)
+            if (roche_by(g, by)) {
+                P.roche_elems += g.count;
+                nr += (g.count + kRocheBlock - 1) / kRocheBlock;
+            }
+        rb[s + 1] = rb[s] + nr;
     }
+    P.eblocks.resize(eb[nseg]);
+    P.ablocks.resize(ab[nseg]);
+    P.rblocks.resize(rb[nseg]);
+    parallel_for(nseg, 64, [&](int64_t s) {
+        const SegDesc& g = P.segs[s];
+        int64_t k = eb[s];
+        for (int64_t off = 0; off < g.count; off += kElemThreads) P.eblocks[k++] = ElemBlock{(int32_t)s, 0, off};
+        k = ab[s];
+        if (g.kind == SEG_STAR1 || g.kind == SEG_STAR2)
+            for (int64_t off = 0; off < g.count; off += kElemThreads) P.ablocks[k++] = ElemBlock{(int32_t)s, 0, off};
+        k = rb[s];
+        for (int by = 1; by <= 2; ++by)
+            if (roche_by(g, by))
+                for (int64_t off = 0; off < g.count; off += kRocheBlock) P.rblocks[k++] = ElemBlock{(int32_t)s, by, off};
+    });
 
     // flux work units: choose the element range so there are a few units per resident block
     int64_t total = 0;
@@ -803,7 +846,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     erange = std::min<int64_t>(std::max<int64_t>(erange, kFluxChunk), 16 * kFluxChunk);
     erange = (erange + kFluxChunk - 1) / kFluxChunk * kFluxChunk;
 
-    std::vector<std::pair<int64_t, FluxUnit>> fu;
+    thread_local std::vector<std::pair<int64_t, FluxUnit>> fu;  // scratch kept across calls
+    fu.clear();
     int64_t pbase = 0;
     for (int64_t i = 0; i < n; ++i) {
         ModelDev& D = lay[i].dev;
@@ -851,9 +895,14 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         pbase += (int64_t)slot * D.nsub;
     }
     P.npartial = pbase;
-    std::stable_sort(fu.begin(), fu.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    P.units.reserve(fu.size());
-    for (auto& x : fu) P.units.push_back(x.second);
+    // largest units first (stable): sort 64-bit keys (descending size, then generation order)
+    thread_local std::vector<uint64_t> order;
+    order.resize(fu.size());
+    for (size_t k = 0; k < fu.size(); ++k)
+        order[k] = ((uint64_t)(INT32_MAX - std::min<int64_t>(fu[k].first, INT32_MAX)) << 32) | (uint64_t)k;
+    std::sort(order.begin(), order.end());
+    P.units.resize(fu.size());
+    for (size_t k = 0; k < fu.size(); ++k) P.units[k] = fu[order[k] & 0xffffffffu].second;
 
     for (int64_t i = 0; i < n; ++i) P.models[i] = lay[i].dev;
 

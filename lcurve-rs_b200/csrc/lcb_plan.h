@@ -27,6 +27,18 @@ struct Plan {
     int64_t evals = 0, roche_elems = 0;
     // Signature of everything that fixes buffer sizes and launch shapes.
     std::vector<int64_t> shape_key;
+    // datum_src[d] == datum_src[0] + d for every d: the data can be copied as one range
+    bool datum_contiguous = false;
+
+    // Empties the plan but keeps every buffer's capacity, so re-planning a
+    // batch of the same size touches no fresh memory.
+    void reset() {
+        models.clear(); segs.clear(); bands.clear(); rings.clear(); eblocks.clear(); rblocks.clear();
+        ablocks.clear(); units.clear(); datum_model.clear(); datum_sub0.clear(); datum_src.clear();
+        model_ok.clear(); model_err.clear(); shape_key.clear();
+        nelem = nsub = ndatum = npartial = evals = roche_elems = 0;
+        datum_contiguous = false;
+    }
 };
 
 // Plans models[0..n); model i is evaluated on data[start[i] .. start[i]+count[i])
