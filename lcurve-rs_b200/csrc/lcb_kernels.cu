@@ -1031,6 +1031,40 @@ struct Contrib {
         else p = a0 + om * (a1 + om * (a2 + om * a3));
         return mu * fl * (1.f - om * p);
     }
+    // Two sub-phases at once with the packed FP32x2 pipe (sm_100): the same
+    // operations as operator(), each lane rounded as its scalar counterpart.
+    __device__ __forceinline__ float2 pair(float2 mu, float fl) const {
+        const float2 one = make_float2(1.f, 1.f), f2 = make_float2(fl, fl);
+        const float2 mf = __fmul2_rn(mu, f2);
+        if (KIND == UK_SPOT) return mf;
+        if (KIND == UK_DISC) {
+            const float2 om = __fadd2_rn(one, make_float2(-mu.x, -mu.y));
+            const float2 q = __ffma2_rn(make_float2(a1, a1), om, make_float2(a0, a0));
+            return __fmul2_rn(mf, __ffma2_rn(make_float2(-om.x, -om.y), q, one));
+        }
+        const float2 m = make_float2(fminf(mu.x, 1.f), fminf(mu.y, 1.f));
+        if (KIND == UK_STAR_CLARET) {
+            const float2 ms = __fmul2_rn(m, make_float2(rsqrtf(m.x), rsqrtf(m.y)));
+            float2 h = __ffma2_rn(ms, make_float2(a3, a3), make_float2(a2, a2));
+            h = __ffma2_rn(ms, h, make_float2(a1, a1));
+            h = __ffma2_rn(ms, h, make_float2(a0, a0));
+            const float2 im = __ffma2_rn(ms, h, make_float2(1.f - sumc, 1.f - sumc));
+            return __fmul2_rn(mf, im);
+        }
+        const float2 om = __fadd2_rn(one, make_float2(-m.x, -m.y));
+        float2 p;
+        if (KIND == UK_STAR_POLY1) p = make_float2(a0, a0);
+        else if (KIND == UK_STAR_POLY2) p = __ffma2_rn(om, make_float2(a1, a1), make_float2(a0, a0));
+        else if (KIND == UK_STAR_POLY3) {
+            p = __ffma2_rn(om, make_float2(a2, a2), make_float2(a1, a1));
+            p = __ffma2_rn(om, p, make_float2(a0, a0));
+        } else {
+            p = __ffma2_rn(om, make_float2(a3, a3), make_float2(a2, a2));
+            p = __ffma2_rn(om, p, make_float2(a1, a1));
+            p = __ffma2_rn(om, p, make_float2(a0, a0));
+        }
+        return __fmul2_rn(mf, __ffma2_rn(make_float2(-om.x, -om.y), p, one));
+    }
 };
 
 // FP32 LDC::imu for the beaming path (types.rs:101-119)
@@ -1103,6 +1137,14 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
     }
     const float sif = (float)M.sini_l, cif = (float)M.cosi_l;
 
+    static_assert(kFluxR % 2 == 0, "sub-phases are processed in pairs");
+    float2 ex2[kFluxR / 2], ey2[kFluxR / 2], ez2[kFluxR / 2];
+#pragma unroll
+    for (int k = 0; k < kFluxR; k += 2) {
+        ex2[k / 2] = make_float2(ex[k], ex[k + 1]);
+        ey2[k / 2] = make_float2(ey[k], ey[k + 1]);
+        ez2[k / 2] = make_float2(ez[k], ez[k + 1]);
+    }
     float acc_hi[kFluxR], acc_lo[kFluxR];
 #pragma unroll
     for (int k = 0; k < kFluxR; ++k) acc_hi[k] = acc_lo[k] = 0.f;
@@ -1187,18 +1229,16 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                             }
                         }
                     }
-                } else if (cls == CLS_VIS) {
-#pragma unroll
-                    for (int k = 0; k < kFluxR; ++k) {
-                        float mu = fmaf(ez[k], r.z, fmaf(ey[k], r.y, ex[k] * r.x));
-                        if (mu > C.thr) part[k] += C(mu, r.w);
-                    }
                 } else {
+                    // sub-phases in pairs on the packed FP32x2 pipe
+                    const float2 rx = make_float2(r.x, r.x), ry = make_float2(r.y, r.y), rz = make_float2(r.z, r.z);
                     const double2* ee = &S.ecl[b][e * kMaxEcl];
 #pragma unroll
-                    for (int k = 0; k < kFluxR; ++k) {
-                        float mu = fmaf(ez[k], r.z, fmaf(ey[k], r.y, ex[k] * r.x));
-                        if (mu > C.thr && !hidden_at(ee, ph[k])) part[k] += C(mu, r.w);
+                    for (int k = 0; k < kFluxR; k += 2) {
+                        const float2 mu = __ffma2_rn(ez2[k / 2], rz, __ffma2_rn(ey2[k / 2], ry, __fmul2_rn(ex2[k / 2], rx)));
+                        const float2 c = C.pair(mu, r.w);
+                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(ee, ph[k]))) part[k] += c.x;
+                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(ee, ph[k + 1]))) part[k + 1] += c.y;
                     }
                 }
             }
