@@ -1,0 +1,59 @@
+"""The multi-rank logic of bench.py on CPU: two gloo ranks.
+
+Each rank evaluates its own batch (weak scaling, seed 1234 + rank); the only
+collective is the timing reduction, the slowest rank's step time; rank 0
+alone runs the reference arm.
+"""
+import importlib
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        import bench
+        ms = [700.0, 950.0][rank]
+        out[rank] = bench.max_over_ranks(ms, "cpu")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_timing_is_the_slowest_rank_and_value_is_weak_scaled():
+    world, port = 2, _free_port()
+    out = mp.Manager().dict()
+    mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
+    assert out[0] == out[1] == 950.0
+    import bench
+    assert bench.weak_value(world, 1024, 950.0) == pytest.approx(2 * 1024 / 0.95)
+    assert bench.max_over_ranks(3.0, "cpu") == 3.0  # no process group: the rank's own value
+
+
+def test_ranks_get_independent_batches():
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    a = W.batch_models(n=4, seed=1234 + 0)
+    b = W.batch_models(n=4, seed=1234 + 1)
+    assert [t for t, _ in a] != [t for t, _ in b]
+
+
+def test_reference_arm_runs_on_rank_0_only(capsys):
+    import bench
+
+    class Args:
+        pass
+    assert bench.run_reference(Args(), rank=1, world=2) is None
+    assert capsys.readouterr().out == ""
