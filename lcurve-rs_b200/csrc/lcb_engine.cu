@@ -61,11 +61,11 @@ struct DevBuf {
 struct DeviceSet {
     DevBuf models, segs, bands, rings, eblocks, rblocks, ablocks, units, dmodel, dsub0, dsrc, data;
     DevBuf rec, pos, p64, d64, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter,
-        datum, ecount;
+        datum, ecount, fcomp, svda;
     void release() {
         for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &rblocks, &ablocks, &units, &dmodel, &dsub0, &dsrc,
                           &data, &rec, &pos, &p64, &d64, &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac,
-                          &partial, &calc, &results, &counter, &datum, &ecount})
+                          &partial, &calc, &results, &counter, &datum, &ecount, &fcomp, &svda})
             b->release();
     }
 };
@@ -162,6 +162,9 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     D.results.ensure(nm * 12 * sizeof(double));
     D.counter.ensure(sizeof(int) * 4);
     D.ecount.ensure(sizeof(unsigned long long) * 8);
+    const size_t ncomp = P.any_iscale ? (size_t)P.ndatum * 5 : 1;
+    D.fcomp.ensure(ncomp * sizeof(double));
+    D.svda.ensure(ncomp * sizeof(double));
 }
 
 // The device launch sequence of one batch evaluation.
@@ -201,7 +204,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     lcb::EpiArgs pe{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dsub0.as<int64_t>(),
                     D.spphi.as<double>(), D.spw.as<double>(), D.slfac.as<double>(), D.partial.as<double>(),
                     D.aux.as<double>(), D.status.as<int>(), scale, rdata, D.calc.as<double>(),
-                    D.results.as<double>(), nm};
+                    D.results.as<double>(), D.fcomp.as<double>(), D.svda.as<double>(), nm};
     CUDA_TRY(lcb::launch_epilogue(pe, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[6], s));
 }
@@ -233,15 +236,11 @@ void fill_result(const double* r, lcb_result* out) {
     for (int k = 0; k < 5; ++k) out->sfac[k] = r[7 + k];
 }
 
-void check_iscale(const lcb::Model& m) {
-    if (m.iscale) throw Error(LCB_ERR_INVALID, "iscale=1 (per-component scale factors) is not supported by this engine yet");
-}
 
 // A transient evaluation on the context's scratch buffers.
 void run_transient(lcb_ctx* C, const lcb::Model* const* models, int64_t n, const lcb_datum* data,
                    const int64_t* start, const int64_t* count, int scale, int rdata, std::vector<double>& res,
                    std::vector<double>* calc, lcb::Plan& P, std::vector<int>& st) {
-    for (int64_t i = 0; i < n; ++i) check_iscale(*models[i]);
     lcb::plan_batch(models, n, data, start, count, C->num_sms, P);
     upload_plan(C, C->scratch, P, data, 0, true);
     enqueue_run(C, C->scratch, P, scale, rdata, false);
@@ -577,7 +576,6 @@ int lcb_batch_create(lcb_ctx* C, const lcb_model* const* models, int64_t nmodels
         B->data.assign(data + offsets[0], data + offsets[0] + total);
         for (int64_t i = 0; i < nmodels; ++i) {
             if (!models[i]) throw Error(LCB_ERR_INVALID, "null model");
-            check_iscale(models[i]->m);
             B->models.push_back(models[i]->m);
             B->start.push_back(offsets[i] - offsets[0]);
             B->count.push_back(offsets[i + 1] - offsets[i]);
@@ -830,6 +828,9 @@ size_t noalloc_carve(const lcb::Plan& P, unsigned char* base, DeviceSet& D) {
     take(D.results, nm * 12 * sizeof(double));
     take(D.counter, sizeof(int) * 4);
     take(D.ecount, sizeof(unsigned long long) * 8);
+    const size_t ncomp = P.any_iscale ? (size_t)P.ndatum * 5 : 1;
+    take(D.fcomp, ncomp * sizeof(double));
+    take(D.svda, ncomp * sizeof(double));
     return off;
 }
 
@@ -863,7 +864,6 @@ extern "C" int lcb_light_curve_noalloc(lcb_ctx* C, const lcb_model* model, const
     if (C->device < 0 || C->device >= kNoallocMaxDevices)
         return fail(LCB_ERR_INVALID, "lcb_light_curve_noalloc: device index beyond the supported 64");
     return guarded(C, [&] {
-        check_iscale(model->m);
         const lcb::Model* mp = &model->m;
         int64_t st = 0, cnt = n;
         lcb::Plan P;

@@ -101,6 +101,7 @@ struct ModelDev {
     int64_t datum_begin, ndatum;    // data
     int64_t pbase;                  // partial buffer offset
     int32_t nslots, g1_end, g2_end, status;  // slots: [0,g1_end) star1, [g1_end,g2_end) star2, rest
+    int32_t gd_end, ge_end;                  // rest: [g2_end,gd_end) disc, [gd_end,ge_end) rim, [ge_end,nslots) spot
 };
 
 struct SegDesc {            // a contiguous run of elements of one model and kind

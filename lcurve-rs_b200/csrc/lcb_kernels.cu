@@ -1325,6 +1325,157 @@ __device__ double block_sum(double v, double* red) {
     return s;
 }
 
+// Several block sums at once (one pair of barriers).
+template <int N>
+__device__ void block_sums(double (&v)[N], double (*red)[kEpiThreads / 32]) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < N; ++k) red[k][warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        double s = 0.0;
+        for (int w = 0; w < kEpiThreads / 32; ++w) s += red[k][w];
+        v[k] = s;
+    }
+}
+
+// iscale = 1 (orchestration.rs:185-227, 264-283, 405-436): the star-1, disc,
+// rim, bright-spot and star-2 fluxes of each datum, and with scale the
+// weighted least-squares scale factor of each, by one-sided Jacobi SVD of
+// the design matrix (singular values at or below 1e-12 dropped), as the
+// oracle restates nalgebra's solve.  No `third` term in this path.
+// comp_star1/2 take the ginterp factor at the exposure's centre phase.
+__device__ void epilogue_iscale(const EpiArgs& A, const ModelDev& M, const Gint& g, double s_wd, const double* aux,
+                                double* res) {
+    __shared__ double red[3][kEpiThreads / 32];
+    const int ncol = M.t2 > 0.0 ? 5 : 4;
+    const double* P = A.partial + M.pbase;
+    double* F = A.fcomp + M.datum_begin * 5;
+    double* X = A.svda + M.datum_begin * 5;
+    for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+        const int64_t gd = M.datum_begin + d;
+        const lcb_datum D = A.data[gd];
+        int64_t j = A.dsub0[gd] - M.sub_begin;
+        const double centre = (D.ndiv > 0 ? A.sp_phi[M.sub_begin + j] : 0.0) +
+                              (D.ndiv > 1 ? 0.5 * D.expose / M.period : 0.0);
+        double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int nd = 0; nd < D.ndiv; ++nd, ++j) {
+            const double w = A.sp_w[M.sub_begin + j];
+            double c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int s = 0; s < M.g1_end; ++s) c[0] += P[(int64_t)s * M.nsub + j];
+            for (int s = M.g2_end; s < M.gd_end; ++s) c[1] += P[(int64_t)s * M.nsub + j];
+            for (int s = M.gd_end; s < M.ge_end; ++s) c[2] += P[(int64_t)s * M.nsub + j];
+            for (int s = M.ge_end; s < M.nslots; ++s) c[3] += P[(int64_t)s * M.nsub + j];
+            for (int s = M.g1_end; s < M.g2_end; ++s) c[4] += P[(int64_t)s * M.nsub + j];
+            f[0] += w * g.scale1(centre) * c[0];
+            f[1] += w * c[1];
+            f[2] += w * c[2];
+            f[3] += w * c[3];
+            f[4] += w * g.scale2(centre) * c[4];
+        }
+        const double den = (double)max(1, D.ndiv - 1), slf = A.d_slfac[gd];
+        for (int k = 0; k < 5; ++k) F[d * 5 + k] = k < ncol ? slf * (f[k] / den) : 0.0;
+    }
+    double sf[5] = {1.0, 1.0, 1.0, 1.0, 1.0}, wdf = 1.0;
+    if (A.scale) {
+        // rows with weight > 0, scaled by sqrt(weight)/ferr; other rows are zero and add nothing
+        double nok[1] = {0.0};
+        for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+            const lcb_datum D = A.data[M.datum_begin + d];
+            const double w = D.weight > 0.0 ? sqrt(D.weight) / D.ferr : 0.0;
+            if (D.weight > 0.0) nok[0] += 1.0;
+            for (int k = 0; k < 5; ++k) X[d * 5 + k] = F[d * 5 + k] * w;
+        }
+        block_sums(nok, red);
+        double x[5] = {1.0, 1.0, 1.0, 1.0, 1.0};
+        if (nok[0] >= ncol && nok[0] > 0.0) {
+            double V[5][5];
+            for (int a = 0; a < 5; ++a)
+                for (int b = 0; b < 5; ++b) V[a][b] = a == b ? 1.0 : 0.0;
+            for (int sweep = 0; sweep < 60; ++sweep) {
+                double off = 0.0;
+                for (int p = 0; p < ncol; ++p)
+                    for (int q = p + 1; q < ncol; ++q) {
+                        double abg[3] = {0.0, 0.0, 0.0};
+                        for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+                            const double ap = X[d * 5 + p], aq = X[d * 5 + q];
+                            abg[0] += ap * ap; abg[1] += aq * aq; abg[2] += ap * aq;
+                        }
+                        block_sums(abg, red);
+                        const double alpha = abg[0], beta = abg[1], gamma = abg[2];
+                        if (gamma == 0.0) continue;
+                        off = fmax(off, fabs(gamma) / sqrt(alpha * beta));
+                        const double zeta = (beta - alpha) / (2.0 * gamma);
+                        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+                        for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+                            const double ap = X[d * 5 + p], aq = X[d * 5 + q];
+                            X[d * 5 + p] = c * ap - s * aq;
+                            X[d * 5 + q] = s * ap + c * aq;
+                        }
+                        for (int i = 0; i < ncol; ++i) {  // every thread keeps the same V
+                            const double vp = V[i][p], vq = V[i][q];
+                            V[i][p] = c * vp - s * vq;
+                            V[i][q] = s * vp + c * vq;
+                        }
+                    }
+                if (off < 1e-15) break;
+            }
+            double sol[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int jc = 0; jc < ncol; ++jc) {
+                double su[2] = {0.0, 0.0};
+                for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+                    const lcb_datum D = A.data[M.datum_begin + d];
+                    const double b = D.weight > 0.0 ? D.flux * sqrt(D.weight) / D.ferr : 0.0;
+                    su[0] += X[d * 5 + jc] * X[d * 5 + jc];
+                    su[1] += X[d * 5 + jc] * b;
+                }
+                block_sums(su, red);
+                const double sj = sqrt(su[0]);
+                if (!(sj > 1e-12)) continue;
+                const double ub = su[1] / sj;
+                for (int k = 0; k < ncol; ++k) sol[k] += V[k][jc] * ub / sj;
+            }
+            bool finite = true;
+            for (int k = 0; k < ncol; ++k) finite = finite && isfinite(sol[k]);
+            if (finite)
+                for (int k = 0; k < ncol; ++k) x[k] = sol[k];
+        }
+        for (int k = 0; k < 5; ++k) sf[k] = k < ncol ? x[k] : 0.0;
+        wdf = x[0];
+    }
+    double cw[2] = {0.0, 0.0};  // chi-squared, wnok
+    for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {
+        const int64_t gd = M.datum_begin + d;
+        const lcb_datum D = A.data[gd];
+        double c = sf[0] * F[d * 5 + 0] + sf[1] * F[d * 5 + 1] + sf[2] * F[d * 5 + 2] + sf[3] * F[d * 5 + 3];
+        if (ncol == 5) c += sf[4] * F[d * 5 + 4];
+        A.calc[gd] = c;
+        if ((A.scale || A.rdata) && D.weight > 0.0) {
+            cw[1] += D.weight;
+            cw[0] += D.weight * sq((D.flux - c) / D.ferr);
+        }
+    }
+    block_sums(cw, red);
+    if (threadIdx.x == 0) {
+        res[0] = s_wd * wdf;
+        res[1] = cw[0];
+        res[2] = cw[1];
+        double fg1 = aux[AUX_FG1], f1 = aux[AUX_F1], fg2 = aux[AUX_FG2], f2 = aux[AUX_F2];
+        res[3] = (M.glogg1 > 0.0 && fg1 > 0.0 && f1 > 0.0) ? log10(M.glogg1 * fg1 / f1) : 0.0;
+        res[4] = (M.glogg2 > 0.0 && fg2 > 0.0 && f2 > 0.0) ? log10(M.glogg2 * fg2 / f2) : 0.0;
+        res[5] = pow(aux[AUX_VOL1] / aux[AUX_SA1], 1.0 / 3.0);
+        res[6] = pow(aux[AUX_VOL2] / aux[AUX_SA2], 1.0 / 3.0);
+        for (int k = 0; k < 5; ++k) res[7 + k] = sf[k];
+    }
+}
+
 __global__ void __launch_bounds__(kEpiThreads) k_epilogue(EpiArgs A) {
     const int64_t m = blockIdx.x;
     const ModelDev& M = A.models[m];
@@ -1357,6 +1508,10 @@ __global__ void __launch_bounds__(kEpiThreads) k_epilogue(EpiArgs A) {
     }
     __syncthreads();
     const Gint g = G;
+    if (M.iscale) {
+        epilogue_iscale(A, M, g, s_wd, aux, res);
+        return;
+    }
     const double* P = A.partial + M.pbase;
     double chi = 0.0, wnok = 0.0, sdy = 0.0, syy = 0.0;
     for (int64_t d = threadIdx.x; d < M.ndatum; d += blockDim.x) {

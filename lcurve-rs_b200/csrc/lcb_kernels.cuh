@@ -68,6 +68,8 @@ struct EpiArgs {
     int scale, rdata;
     double* calc;        // per datum
     double* results;     // 12 per model
+    double* fcomp;       // iscale: 5 component fluxes per datum
+    double* svda;        // iscale: 5 per datum, the weighted design matrix of the scale fit
     int64_t nmodels;
 };
 

@@ -852,7 +852,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     for (int64_t i = 0; i < n; ++i) {
         ModelDev& D = lay[i].dev;
         D.pbase = pbase;
-        if (!P.model_ok[i] || D.nsub == 0) { D.nslots = D.g1_end = D.g2_end = 0; continue; }
+        if (!P.model_ok[i] || D.nsub == 0) { D.nslots = D.g1_end = D.g2_end = D.gd_end = D.ge_end = 0; continue; }
         int32_t slot = 0;
         auto kind_of = [&](const SegDesc& g) {
             if (g.kind == SEG_DISC || g.kind == SEG_EDGE) return (int32_t)UK_DISC;
@@ -865,10 +865,13 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             int np = s1 ? D.npoly1 : D.npoly2;
             return (int32_t)(UK_STAR_POLY1 + (np - 1));
         };
-        for (int pass = 0; pass < 3; ++pass) {  // star1 slots, star2 slots, the rest
+        // slots grouped by component: star 1, star 2, disc, rim, bright spot
+        // (the per-component sums of iscale read them as contiguous ranges)
+        for (int pass = 0; pass < 5; ++pass) {
             for (size_t s = seg_begin[i]; s < seg_begin[i + 1]; ++s) {
                 const SegDesc& g = P.segs[s];
-                int grp = g.kind == SEG_STAR1 ? 0 : g.kind == SEG_STAR2 ? 1 : 2;
+                int grp = g.kind == SEG_STAR1 ? 0 : g.kind == SEG_STAR2 ? 1 : g.kind == SEG_DISC ? 2
+                          : g.kind == SEG_EDGE ? 3 : 4;
                 if (grp != pass) continue;
                 for (int64_t e = 0; e < g.count; e += erange) {
                     int32_t ne = (int32_t)std::min<int64_t>(erange, g.count - e);
@@ -890,6 +893,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             }
             if (pass == 0) D.g1_end = slot;
             if (pass == 1) D.g2_end = slot;
+            if (pass == 2) D.gd_end = slot;
+            if (pass == 3) D.ge_end = slot;
         }
         D.nslots = slot;
         pbase += (int64_t)slot * D.nsub;
@@ -904,7 +909,10 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     P.units.resize(fu.size());
     for (size_t k = 0; k < fu.size(); ++k) P.units[k] = fu[order[k] & 0xffffffffu].second;
 
-    for (int64_t i = 0; i < n; ++i) P.models[i] = lay[i].dev;
+    for (int64_t i = 0; i < n; ++i) {
+        P.models[i] = lay[i].dev;
+        P.any_iscale = P.any_iscale || (P.model_ok[i] && lay[i].dev.iscale);
+    }
 
     // shape key: what the device buffers and the captured graph depend on
     P.shape_key = {n, P.nelem, P.nsub, P.ndatum, P.npartial, (int64_t)P.units.size(), (int64_t)P.eblocks.size(),

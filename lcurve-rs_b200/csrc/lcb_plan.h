@@ -29,6 +29,7 @@ struct Plan {
     std::vector<int64_t> shape_key;
     // datum_src[d] == datum_src[0] + d for every d: the data can be copied as one range
     bool datum_contiguous = false;
+    bool any_iscale = false;  // some model fits per-component scale factors (needs fcomp scratch)
 
     // Empties the plan but keeps every buffer's capacity, so re-planning a
     // batch of the same size touches no fresh memory.
@@ -38,6 +39,7 @@ struct Plan {
         model_ok.clear(); model_err.clear(); shape_key.clear();
         nelem = nsub = ndatum = npartial = evals = roche_elems = 0;
         datum_contiguous = false;
+        any_iscale = false;
     }
 };
 

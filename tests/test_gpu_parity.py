@@ -152,3 +152,34 @@ def test_ragged_batch_and_resident_batch_vs_oracle(lcb, oracle, W):
         om.set("q", q[i])
         c = om.light_curve(data[offs[i]:offs[i + 1]], rdata=True, nthreads=8)["chisq"]
         assert abs(bchi3[i] - c) <= 1e-4 * abs(c)
+
+
+@pytest.mark.parametrize("scale", [False, True])
+def test_iscale_components_and_svd_scale_vs_oracle(lcb, oracle, W, scale):
+    """iscale = 1: per-component fluxes (star 1, disc, rim, spot, star 2) and,
+    with scale, the least-squares factor of each component (one-sided Jacobi
+    SVD, restated by the oracle; no reference test pins nalgebra's result).
+    Tolerances: fluxes 1e-5 relative, scale factors and chi-squared 1e-4
+    relative (the fit amplifies the FP32 flux sum's rounding by the design
+    matrix's conditioning)."""
+    o = dict(W.SMALL)
+    o.update(nlat1f=40, nlat1c=40, nlat2f=80, nlat2c=80, add_disc=1, opaque=1, rdisc1=0.02, rdisc2=0.3,
+             texp_disc=-0.75, nrad=50, add_spot=1, temp_spot=12000.0, length_spot=0.05, expon_spot=0.0,
+             epow_spot=2.0, nspot=40, absorb=0.5, iscale=1)
+    text = W.model_text(**o)
+    t = np.linspace(-0.2, 1.2, 900)
+    # data: the model's own curve with different weights on its components, 1% noise
+    base = oracle.Model(text=text).light_curve(lcb.make_data(t, expose=0.01, ndiv=3), scale=False)["calc"]
+    rng = np.random.default_rng(5)
+    flux = base * (1.0 + 0.1 * np.sin(3.0 * t)) * (1.0 + 0.01 * rng.standard_normal(t.size))
+    d = lcb.make_data(t, expose=0.01, ndiv=3, flux=flux, ferr=0.01 * np.abs(flux), weight=1.0)
+    d["weight"][::17] = 0.0  # some points out of the fit
+    calc, res, o_ = gpu_and_oracle_lc(lcb, oracle, text, t, 0.01, 3, scale=scale, rdata=True, data=d)
+    assert rel_err(calc, o_["calc"]) < TOL
+    tol = 1e-4
+    assert np.allclose(list(res.sfac), o_["sfac"], rtol=tol, atol=0), (list(res.sfac), o_["sfac"])
+    assert res.chisq == pytest.approx(o_["chisq"], rel=tol)
+    assert res.wnok == o_["wnok"]
+    assert res.wdwarf == pytest.approx(o_["wdwarf"], rel=tol)
+    if scale:
+        assert not np.allclose(o_["sfac"], 1.0)  # the fit moved the factors
