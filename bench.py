@@ -227,7 +227,7 @@ def run_mcmc(args, lcb):
     samplers started from one burned-in ensemble; ESS/s over the sampling
     loops.  Plain samplers: the stretch move (the reference fitter's emcee
     default) and the KDE move; the delayed-acceptance sampler screens KDE
-    moves with the surrogate (and, in --mcmc-full, stretch sub-chains too)."""
+    moves with the surrogate."""
     S = importlib.import_module("lcurve-rs_b200.surrogate")
     M = importlib.import_module("lcurve-rs_b200.mcmc")
     W = importlib.import_module("lcurve-rs_b200.workloads")
@@ -255,8 +255,6 @@ def run_mcmc(args, lcb):
         "plain_kde": M.run_plain(eng, start, args.mcmc_steps, seed=5, move="kde", bandwidth=bw),
         "da_kde": M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=k, move="kde", bandwidth=bw),
     }
-    if args.mcmc_full:
-        runs["da_stretch"] = M.run_delayed(eng, sur, start, args.mcmc_steps, seed=5, substeps=32)
     ess = {name: M.ess(r, burn=0.0) for name, r in runs.items()}
     rate = {name: ess[name][0] / r.seconds for name, r in runs.items()}
     post = {name: M.posterior_summary(r, burn=0.0) for name, r in runs.items()}
