@@ -927,10 +927,12 @@ enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
 struct FluxSmem {
     float4 rec[2][kFluxChunk];
     double2 ecl[2][kFluxChunk * kMaxEcl];
-    int8_t cls[kFluxChunk];
+    uint16_t list[kFluxChunk];   // contributing elements of the chunk: index | (partly eclipsed << 15)
+    int wtot[2][kFluxThreads / 32];
     uint64_t bar[2];
     int unit;
 };
+static_assert(kFluxChunk == 2 * kFluxThreads, "the classification pass gives each thread two elements");
 
 size_t flux_smem_bytes_impl() { return sizeof(FluxSmem); }
 
@@ -1180,23 +1182,54 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         const int n = min(kFluxChunk, U.ne - c * kFluxChunk);
         if (!mbar_wait(&S.bar[b], parity[b])) atomicOr(A.status + U.model, kStatusTmaTimeout);
         parity[b] ^= 1u;
-        for (int e = tid; e < n; e += kFluxThreads) {
-            int cl = classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
-            if (cl != CLS_HID) {  // never facing the observer on this tile: contributes exactly 0
-                const float4 r = S.rec[b][e];
-                if (max_mu(arcs, sif, cif, r.x, r.y, r.z) <= face_thr) cl = CLS_HID;
+        // classify every element of the chunk and list the contributing ones in
+        // ascending order (ballot prefix sums): the loop below then runs over a
+        // dense list without per-element branches
+        const int lane = tid & 31, warp = tid >> 5;
+        uint16_t ent[2];
+        unsigned keep[2];
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+            const int e = tid + rr * kFluxThreads;
+            int cl = CLS_HID;
+            if (e < n) {
+                cl = classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
+                if (cl != CLS_HID) {  // never facing the observer on this tile: contributes exactly 0
+                    const float4 r = S.rec[b][e];
+                    if (max_mu(arcs, sif, cif, r.x, r.y, r.z) <= face_thr) cl = CLS_HID;
+                }
             }
-            S.cls[e] = (int8_t)cl;
+            ent[rr] = (uint16_t)(e | (cl == CLS_MIX ? 0x8000 : 0));
+            keep[rr] = __ballot_sync(0xffffffffu, cl != CLS_HID);
+            if (lane == 0) S.wtot[rr][warp] = __popc(keep[rr]);
         }
         __syncthreads();
-        for (int s0 = 0; s0 < n; s0 += 32) {
+        int nlist = 0;
+        {
+            const unsigned below = (1u << lane) - 1u;
+            int base = 0;
+#pragma unroll
+            for (int rr = 0; rr < 2; ++rr) {
+                int off = base;
+                for (int w = 0; w < kFluxThreads / 32; ++w) {
+                    if (w == warp) off = base;
+                    base += S.wtot[rr][w];
+                }
+                if ((keep[rr] >> lane) & 1u) S.list[off + __popc(keep[rr] & below)] = ent[rr];
+            }
+            nlist = base;
+        }
+        __syncthreads();
+        for (int s0 = 0; s0 < nlist; s0 += 32) {
             float part[kFluxR];
 #pragma unroll
             for (int k = 0; k < kFluxR; ++k) part[k] = 0.f;
-            const int s1 = min(s0 + 32, n);
-            for (int e = s0; e < s1; ++e) {
-                const int cls = S.cls[e];
-                if (cls == CLS_HID) continue;
+            const int s1 = min(s0 + 32, nlist);
+#pragma unroll 2
+            for (int q = s0; q < s1; ++q) {
+                const int ev = S.list[q];
+                const int e = ev & 0x7fff;
+                const int cls = (ev & 0x8000) ? CLS_MIX : CLS_VIS;
                 const float4 r = S.rec[b][e];
                 if (KIND == UK_STAR_GENERIC) {
                     const float4 p = __ldg(A.el_pos + U.e0 + (int64_t)c * kFluxChunk + e);
