@@ -161,7 +161,10 @@ constexpr int kFluxR = 4;                          // sub-phases per thread
 constexpr int kFluxTile = kFluxThreads * kFluxR;   // sub-phases per work unit
 constexpr int kFluxChunk = 256;                    // elements staged per TMA chunk
 constexpr int kElemThreads = 256;
-constexpr int kRocheBlock = 128;                   // elements per k_roche block
+#ifndef LCB_ROCHE_BLOCK
+#define LCB_ROCHE_BLOCK 128
+#endif
+constexpr int kRocheBlock = LCB_ROCHE_BLOCK;       // elements per k_roche block
 
 // Device status bits (ModelDev.status / batch status word).
 constexpr int kStatusIterCap = 1;     // an iteration cap without a reference counterpart tripped
