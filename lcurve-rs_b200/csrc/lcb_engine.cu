@@ -61,11 +61,11 @@ struct DevBuf {
 struct DeviceSet {
     DevBuf models, segs, bands, rings, eblocks, rblocks, ablocks, units, dmodel, dsub0, dsrc, data;
     DevBuf rec, pos, p64, d64, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter,
-        datum, ecount, fcomp, svda;
+        datum, ecount, fcomp, svda, firsthit;
     void release() {
         for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &rblocks, &ablocks, &units, &dmodel, &dsub0, &dsrc,
                           &data, &rec, &pos, &p64, &d64, &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac,
-                          &partial, &calc, &results, &counter, &datum, &ecount, &fcomp, &svda})
+                          &partial, &calc, &results, &counter, &datum, &ecount, &fcomp, &svda, &firsthit})
             b->release();
     }
 };
@@ -165,6 +165,7 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     const size_t ncomp = P.any_iscale ? (size_t)P.ndatum * 5 : 1;
     D.fcomp.ensure(ncomp * sizeof(double));
     D.svda.ensure(ncomp * sizeof(double));
+    D.firsthit.ensure((P.roche_split > 1 ? P.rblocks.size() * lcb::kRocheBlock : 1) * sizeof(int));
 }
 
 // The device launch sequence of one batch evaluation.
@@ -186,7 +187,9 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
                      D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
                      D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
                      (int64_t)P.eblocks.size(), (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(),
-                     D.ecount.as<unsigned long long>()};
+                     D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>()};
+    if (P.roche_split > 1)
+        CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, P.rblocks.size() * lcb::kRocheBlock * sizeof(int), s));
     CUDA_TRY(lcb::launch_elements(ea, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[2], s));
     CUDA_TRY(lcb::launch_roche(ea, s));
@@ -831,6 +834,7 @@ size_t noalloc_carve(const lcb::Plan& P, unsigned char* base, DeviceSet& D) {
     const size_t ncomp = P.any_iscale ? (size_t)P.ndatum * 5 : 1;
     take(D.fcomp, ncomp * sizeof(double));
     take(D.svda, ncomp * sizeof(double));
+    take(D.firsthit, (P.roche_split > 1 ? P.rblocks.size() * lcb::kRocheBlock : 1) * sizeof(int));
     return off;
 }
 

@@ -336,18 +336,42 @@ __device__ bool sphere_phase(double cosi, double sini, double px, double py, dou
 // site: lanes of a warp in different stages reconverge inside the search, and
 // the search code exists once.  Misses are proven (fblink's `prove`) only in the
 // scan, where nearly all lines of sight miss by a wide margin.
+// The phase scan of pot_min_search (eclipse.rs:347-373): phases phi1 + i dphi,
+// i = 0 .. nsteps, and the search tolerance acc (eclipse.rs:297).
+struct Scan {
+    double phi1, phi2, acc, dphi;
+    int nsteps;
+};
+__device__ __forceinline__ bool scan_setup(const RocheEcl& s, double cosi, double sini, double delta, double px,
+                                           double py, double pz, Scan& sc) {
+    double lam1, lam2;
+    if (!sphere_phase(cosi, sini, px, py, pz, s.cofmx, s.rref, sc.phi1, sc.phi2, lam1, lam2)) return false;
+    sc.acc = 2.0 * sqrt(2.0 * kTwoPi * (lam2 - lam1) * delta);
+    double ns = ceil((sc.phi2 - sc.phi1) / (sc.acc / kTwoPi));
+    sc.nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
+    sc.dphi = (sc.phi2 - sc.phi1) / (double)sc.nsteps;
+    return true;
+}
+
+constexpr int kNoHit = 0x7f7f7f7f;  // first-hit sentinel (the byte pattern a memset of 0x7f writes)
+
+// `known_hit` >= 0: the scan's first hit is already known (split scan): go
+// straight to the bisections from that phase; kNoHit: the point is not eclipsed.
 __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
-                               double pz, double& ing, double& eg, bool& capped, EclCount& evals) {
-    double phi1, phi2, lam1, lam2;
-    if (!sphere_phase(cosi, sini, px, py, pz, s.cofmx, s.rref, phi1, phi2, lam1, lam2)) return false;
-    double acc = 2.0 * sqrt(2.0 * kTwoPi * (lam2 - lam1) * delta);
+                               double pz, double& ing, double& eg, bool& capped, EclCount& evals, int known_hit = -1) {
+    Scan sc;
+    if (!scan_setup(s, cosi, sini, delta, px, py, pz, sc)) return false;
+    if (known_hit == kNoHit) return false;
+    const double phi1 = sc.phi1, phi2 = sc.phi2, acc = sc.acc, dphi = sc.dphi;
+    const int nsteps = sc.nsteps;
     Los L{px, py, pz, 0.0, 0.0, 0.0};
-    double ns = ceil((phi2 - phi1) / (acc / kTwoPi));
-    const int nsteps = (ns != ns || ns <= 10.0) ? 10 : (ns >= 1000.0 ? 1000 : (int)ns);
-    const double dphi = (phi2 - phi1) / (double)nsteps;
     enum { SCAN, CHOP_IN, CHOP_EG };
     int mode = SCAN, i = 0, it = 0;
     double phi = 0.0, pin = 0.0, pout = 0.0;
+    if (known_hit >= 0) {  // as the scan below sets up its first hit
+        phi = phi1 + (double)known_hit * dphi;
+        mode = CHOP_IN; pin = phi; pout = phi1;
+    }
     for (;;) {
         double ph;
         if (mode == SCAN) {
@@ -736,6 +760,8 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
 // ---------------------------------------------------------------------------
 // k_roche: FP64 Roche ray-march of one element per thread (eclipse.rs:270-373)
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void roche_counters(const ElemArgs& A, const EclCount& cnt);
+
 __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs A) {
     const ElemBlock blk = A.rblocks[blockIdx.x];
     const SegDesc sg = A.segs[blk.seg];
@@ -752,16 +778,87 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs
             A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, by)] = make_double2(a, b);
         if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
     }
-    if (A.counters) {  // eclipse-search work counters, one atomic per warp and counter
-        unsigned long long v[5] = {(unsigned long long)cnt.pot, (unsigned long long)cnt.dpot,
-                                   (unsigned long long)cnt.fbl, (unsigned long long)cnt.cert,
-                                   (unsigned long long)cnt.skipped};
-        for (int k = 0; k < 5; ++k) {
-            unsigned long long x = v[k];
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if ((threadIdx.x & 31) == 0 && x) atomicAdd(A.counters + k, x);
+    roche_counters(A, cnt);
+}
+
+// One chunk of a split phase scan: scan indices [c L, (c+1) L) of 0 .. nsteps,
+// L = ceil((nsteps+1)/K); the first hit is merged into *first with atomicMin,
+// and a chunk stops once an earlier chunk has hit.  The minimum over chunks is
+// the single scan's first hit, so the decision is the reference's.
+__device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
+                           double pz, int chunk, int split, int* first, bool& capped, EclCount& evals) {
+    Scan sc;
+    if (!scan_setup(s, cosi, sini, delta, px, py, pz, sc)) return;
+    const int total = sc.nsteps + 1, len = (total + split - 1) / split;
+    const int lo = chunk * len, hi = min(total, lo + len);
+    Los L{px, py, pz, 0.0, 0.0, 0.0};
+    for (int i = lo; i < hi; ++i) {
+        if (((i - lo) & 7) == 0 && *(volatile int*)first < lo) return;
+        earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
+        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget > 0);
+        if (capped) return;
+        if (hit) {
+            atomicMin(first, i);
+            return;
         }
     }
+}
+
+__device__ __forceinline__ void roche_counters(const ElemArgs& A, const EclCount& cnt) {
+    if (!A.counters) return;  // eclipse-search work counters, one atomic per warp and counter
+    unsigned long long v[5] = {(unsigned long long)cnt.pot, (unsigned long long)cnt.dpot, (unsigned long long)cnt.fbl,
+                               (unsigned long long)cnt.cert, (unsigned long long)cnt.skipped};
+    for (int k = 0; k < 5; ++k) {
+        unsigned long long x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(A.counters + k, x);
+    }
+}
+
+// Split scan, first kernel: block b scans chunk b % split of the elements of
+// Roche block b / split.  For small batches, whose time is otherwise the
+// longest single scan, this spreads each scan over `split` threads.
+__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(ElemArgs A) {
+    const int64_t rb = blockIdx.x / A.roche_split;
+    const int chunk = (int)(blockIdx.x % A.roche_split);
+    const ElemBlock blk = A.rblocks[rb];
+    const SegDesc sg = A.segs[blk.seg];
+    const int64_t i = blk.offset + threadIdx.x;
+    EclCount cnt;
+    bool capped = false;
+    if (i < sg.count) {
+        const ModelDev& M = A.models[sg.model];
+        const double4 p = A.el_p64[sg.first + i];
+        scan_chunk(blk.by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, chunk, A.roche_split,
+                   A.firsthit + rb * kRocheBlock + threadIdx.x, capped, cnt);
+        if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
+    }
+    cnt.fbl = 0;  // the second kernel counts the reference's scan searches
+    roche_counters(A, cnt);
+}
+
+// Split scan, second kernel: the bisections from the first hit.
+__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop(ElemArgs A) {
+    const ElemBlock blk = A.rblocks[blockIdx.x];
+    const SegDesc sg = A.segs[blk.seg];
+    const int64_t i = blk.offset + threadIdx.x;
+    EclCount cnt;
+    bool capped = false;
+    if (i < sg.count) {
+        const ModelDev& M = A.models[sg.model];
+        const RocheEcl& R = blk.by == 1 ? M.ecl1 : M.ecl2;
+        const int64_t e = sg.first + i;
+        const double4 p = A.el_p64[e];
+        const int first = A.firsthit[(int64_t)blockIdx.x * kRocheBlock + threadIdx.x];
+        Scan sc;
+        if (scan_setup(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, sc))
+            cnt.fbl += first == kNoHit ? sc.nsteps + 1 : first + 1;  // the single scan's searches
+        double a, b;
+        if (ingress_egress(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt, first))
+            A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, blk.by)] = make_double2(a, b);
+        if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
+    }
+    roche_counters(A, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1697,7 +1794,15 @@ cudaError_t launch_elements(const ElemArgs& a, cudaStream_t s) {
 
 cudaError_t launch_roche(const ElemArgs& a, cudaStream_t s) {
     if (a.nrblocks <= 0) return cudaSuccess;
-    k_roche<<<(unsigned)a.nrblocks, kRocheBlock, 0, s>>>(a);
+    if (a.roche_split <= 1) {
+        k_roche<<<(unsigned)a.nrblocks, kRocheBlock, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+    // firsthit starts at kNoHit (memset by the caller's launch sequence)
+    k_roche_scan<<<(unsigned)(a.nrblocks * a.roche_split), kRocheBlock, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_roche_chop<<<(unsigned)a.nrblocks, kRocheBlock, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,8 @@ struct ElemArgs {
     int* status;         // per model
     int64_t nblocks, nrblocks, nablocks;
     unsigned long long* counters;  // [pot evals, dpot evals, fblink calls, bound nodes, proven misses] or null
+    int roche_split;     // threads per Roche-eclipsed element in the phase scan (1: one kernel)
+    int* firsthit;       // split scan: first hit per Roche thread (nrblocks x kRocheBlock), starts at 0x7f7f7f7f
 };
 
 struct PhaseArgs {

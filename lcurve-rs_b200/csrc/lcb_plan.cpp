@@ -836,6 +836,14 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
                 for (int64_t off = 0; off < g.count; off += kRocheBlock) P.rblocks[k++] = ElemBlock{(int32_t)s, by, off};
     });
 
+    // small batches: spread each element's phase scan over several threads until
+    // about two waves of Roche blocks fill the GPU (large batches keep one)
+    {
+        const int64_t threads = (int64_t)P.rblocks.size() * kRocheBlock;
+        const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 2;
+        P.roche_split = threads > 0 ? (int)std::min<int64_t>(std::max<int64_t>(target / threads, 1), 16) : 1;
+    }
+
     // flux work units: choose the element range so there are a few units per resident block
     int64_t total = 0;
     for (const SegDesc& g : P.segs) total += g.count * lay[g.model].dev.nsub;
@@ -917,7 +925,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     // shape key: what the device buffers and the captured graph depend on
     P.shape_key = {n, P.nelem, P.nsub, P.ndatum, P.npartial, (int64_t)P.units.size(), (int64_t)P.eblocks.size(),
                    (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(), (int64_t)P.segs.size(),
-                   (int64_t)P.bands.size(), (int64_t)P.rings.size()};
+                   (int64_t)P.bands.size(), (int64_t)P.rings.size(), (int64_t)P.roche_split};
 }
 
 }  // namespace lcb

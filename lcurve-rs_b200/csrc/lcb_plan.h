@@ -30,6 +30,7 @@ struct Plan {
     // datum_src[d] == datum_src[0] + d for every d: the data can be copied as one range
     bool datum_contiguous = false;
     bool any_iscale = false;  // some model fits per-component scale factors (needs fcomp scratch)
+    int roche_split = 1;      // threads per Roche-eclipsed element in the phase scan
 
     // Empties the plan but keeps every buffer's capacity, so re-planning a
     // batch of the same size touches no fresh memory.
@@ -40,6 +41,7 @@ struct Plan {
         nelem = nsub = ndatum = npartial = evals = roche_elems = 0;
         datum_contiguous = false;
         any_iscale = false;
+        roche_split = 1;
     }
 };
 
