@@ -837,10 +837,10 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     });
 
     // small batches: spread each element's phase scan over several threads until
-    // about two waves of Roche blocks fill the GPU (large batches keep one)
+    // about four waves of Roche blocks fill the GPU (large batches keep one)
     {
         const int64_t threads = (int64_t)P.rblocks.size() * kRocheBlock;
-        const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 2;
+        const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 4;
         P.roche_split = threads > 0 ? (int)std::min<int64_t>(std::max<int64_t>(target / threads, 1), 16) : 1;
     }
 
