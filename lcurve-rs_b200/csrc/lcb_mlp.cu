@@ -5,7 +5,7 @@
 // t1, t2, normalised by the caller) to a light curve on a fixed phase grid
 // (standardised log fluxes): n_in -> width x n_hidden (GELU) -> n_out.  It is
 // the cheap first stage of delayed-acceptance MCMC; the light-curve engine
-// stays the second-stage judge.
+// stays the second stage that decides every move.
 //
 // GEMM kernel (k_gemm): C[M x N] = A[M x K] . B[N x K]^T, both operands BF16
 // row-major (K contiguous), FP32 accumulation in tensor memory:

@@ -17,7 +17,7 @@ posterior alone,
            l~ = surrogate log probability,
 
 which is a kernel reversible with respect to the surrogate posterior; only a
-walker whose sub-chain moved it from x to y is then judged by the engine,
+walker whose sub-chain moved it from x to y is then decided by the engine,
 
   stage 2  accept y with min(1, exp(l(y) - l(x) - l~(y) + l~(x)))
            l = engine log probability,
@@ -29,7 +29,7 @@ With substeps = 1 this is Christen & Fox's two-stage
 delayed acceptance; with more sub-steps it is the surrogate transition method
 (Liu 2001, sec. 9.4.3).  Either way the pair of stages satisfies detailed
 balance with respect to the engine's posterior, so both samplers target the
-same distribution and the engine judges every accepted move.
+same distribution and the engine decides every accepted move.
 """
 from __future__ import annotations
 
@@ -227,7 +227,7 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
                 y, lsy = subchain_host(surrogate, x[S], lps[S], x[Cc], rnd, a, move=move, bandwidth=bandwidth)
             nsur += substeps * len(S)
             moved = np.any(y != x[S], axis=1)
-            # stage 2: the engine judges the walkers that moved
+            # stage 2: the engine decides for the walkers that moved
             if moved.any():
                 idx = np.nonzero(moved)[0]
                 lpy = log_prior(y[idx]) + _eval_engine(engine, y[idx])
