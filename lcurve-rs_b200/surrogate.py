@@ -311,16 +311,39 @@ class Surrogate:
         else:
             chol = prec = None
             keep = ()
+        comp = np.ascontiguousarray(comp, dtype=np.float64)
+        m = comp.shape[0]
+        # one pinned staging buffer, one copy each way: [y (n x d), ls (n), comp (m x d), rnd]
+        sizes = (n * d, n, m * d, rnd.size)
+        offs = np.cumsum((0,) + sizes)
+        buf_h, buf_d = self._staging(int(offs[-1]))
+        h = buf_h.numpy()
+        h[offs[0]:offs[1]] = y.ravel()
+        h[offs[1]:offs[2]] = ls
+        h[offs[2]:offs[3]] = comp.ravel()
+        h[offs[3]:offs[4]] = np.asarray(rnd, dtype=np.float64).ravel()
+        base = buf_d.data_ptr()
+        ptr = [C.c_void_p(base + 8 * int(o)) for o in offs[:4]]
         with torch.cuda.stream(self._stream):
-            yd = torch.as_tensor(y).to(self.dev)
-            lsd = torch.as_tensor(np.ascontiguousarray(ls, dtype=np.float64)).to(self.dev)
-            cd = torch.as_tensor(np.ascontiguousarray(comp, dtype=np.float64)).to(self.dev)
-            rd = torch.as_tensor(np.ascontiguousarray(rnd, dtype=np.float64)).to(self.dev)
+            buf_d[:offs[4]].copy_(buf_h[:offs[4]], non_blocking=True)
             _capi.check_mlp(self.L.lcb_surrogate_subchain(
-                self._h, n, cd.shape[0], d, C.c_void_p(yd.data_ptr()), C.c_void_p(lsd.data_ptr()),
-                C.c_void_p(cd.data_ptr()), C.c_void_p(rd.data_ptr()), rnd.shape[0], a, self._c_lo, self._c_hi,
+                self._h, n, m, d, ptr[0], ptr[1], ptr[2], ptr[3], rnd.shape[0], a, self._c_lo, self._c_hi,
                 self._c_recip, self._c_fmul, self._c_fadd, C.c_void_p(self.mean.data_ptr()),
                 C.c_void_p(self.sd.data_ptr()), C.c_void_p(self._flux.data_ptr()), C.c_void_p(self._ferr.data_ptr()),
                 int(bool(scale)), 1 if move == "kde" else 0, chol, prec))
-            del keep
-            return yd.cpu().numpy(), lsd.cpu().numpy()
+            out = self._out_h[:offs[2]]
+            out.copy_(buf_d[:offs[2]], non_blocking=True)
+        self._stream.synchronize()
+        del keep
+        o = out.numpy()
+        return o[:n * d].reshape(n, d).copy(), o[n * d:n * d + n].copy()
+
+    def _staging(self, count: int):
+        """Pinned host and device buffers of at least `count` doubles (kept across calls)."""
+        torch = _torch()
+        if getattr(self, "_stage_n", 0) < count:
+            self._stage_n = max(count, 2 * getattr(self, "_stage_n", 0))
+            self._stage_h = torch.empty(self._stage_n, dtype=torch.float64, pin_memory=True)
+            self._stage_d = torch.empty(self._stage_n, dtype=torch.float64, device=self.dev)
+            self._out_h = torch.empty(self._stage_n, dtype=torch.float64, pin_memory=True)
+        return self._stage_h, self._stage_d
