@@ -908,14 +908,26 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         pbase += (int64_t)slot * D.nsub;
     }
     P.npartial = pbase;
-    // largest units first (stable): sort 64-bit keys (descending size, then generation order)
-    thread_local std::vector<uint64_t> order;
-    order.resize(fu.size());
-    for (size_t k = 0; k < fu.size(); ++k)
-        order[k] = ((uint64_t)(INT32_MAX - std::min<int64_t>(fu[k].first, INT32_MAX)) << 32) | (uint64_t)k;
-    std::sort(order.begin(), order.end());
-    P.units.resize(fu.size());
-    for (size_t k = 0; k < fu.size(); ++k) P.units[k] = fu[order[k] & 0xffffffffu].second;
+    // largest units first, ties in generation order: a stable two-pass radix sort
+    // (16 bits each) of the 32-bit keys INT32_MAX - size
+    thread_local std::vector<uint32_t> key, idx, tmp;
+    const size_t nu = fu.size();
+    key.resize(nu);
+    idx.resize(nu);
+    tmp.resize(nu);
+    for (size_t k = 0; k < nu; ++k) {
+        key[k] = (uint32_t)(INT32_MAX - std::min<int64_t>(fu[k].first, INT32_MAX));
+        idx[k] = (uint32_t)k;
+    }
+    for (int shift = 0; shift < 32; shift += 16) {
+        std::vector<size_t> count(65537, 0);
+        for (size_t k = 0; k < nu; ++k) ++count[((key[idx[k]] >> shift) & 0xffffu) + 1];
+        for (size_t b = 1; b < count.size(); ++b) count[b] += count[b - 1];
+        for (size_t k = 0; k < nu; ++k) tmp[count[(key[idx[k]] >> shift) & 0xffffu]++] = idx[k];
+        idx.swap(tmp);
+    }
+    P.units.resize(nu);
+    for (size_t k = 0; k < nu; ++k) P.units[k] = fu[idx[k]].second;
 
     for (int64_t i = 0; i < n; ++i) {
         P.models[i] = lay[i].dev;
