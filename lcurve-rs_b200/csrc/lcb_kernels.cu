@@ -1322,7 +1322,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll
             for (int k = 0; k < kFluxR; ++k) part[k] = 0.f;
             const int s1 = min(s0 + 32, nlist);
-#pragma unroll 2
+#pragma unroll 4
             for (int q = s0; q < s1; ++q) {
                 const int ev = S.list[q];
                 const int e = ev & 0x7fff;
