@@ -53,14 +53,22 @@ namespace {
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4, GEMM_THREADS = 128;
-constexpr uint32_t TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
+// Tiles: 128 rows x TBN columns (TBN = 256 when N allows: half the CTAs, the
+// widest single-CTA MMA; 128 otherwise), K-slices of 64.
+// 16 warps: warp 0 lane 0 issues the TMA copies, warp 1 lane 0 the MMAs; in the epilogue warp w
+// reads TMEM lanes 32 (w % 4) .. + 31 (the quarter its warp id may access) and the column
+// chunks w / 4, w / 4 + 4, ... of 32.
+constexpr int BM = 128, BK = 64, STAGES = 4, GEMM_THREADS = 512, EPI_GROUPS = GEMM_THREADS / 128;
+constexpr uint32_t TILE_A = BM * BK * 2;
+template <int TBN>
+__host__ __device__ constexpr uint32_t tile_b() { return (uint32_t)TBN * BK * 2; }
 
 enum { EPI_F32 = 0, EPI_BIAS_GELU = 1, EPI_BIAS_F32 = 2, EPI_DGELU = 3 };
 
+template <int TBN>
 struct GemmSmem {
     uint8_t a[STAGES][TILE_A];  // 1024-byte aligned slices (128-byte swizzle atoms)
-    uint8_t b[STAGES][TILE_B];
+    uint8_t b[STAGES][tile_b<TBN>()];
     uint64_t full[STAGES], empty[STAGES], done;
     uint32_t tmem_base;
     int abort;
@@ -68,10 +76,13 @@ struct GemmSmem {
 
 struct GemmArgs {
     int M, N, K;
+    int kchunks;      // BK-chunks of K per split (blockIdx.z); all of K when not split
+    int64_t zstride;  // elements between the FP32 outputs of consecutive splits
     const float* bias;
     const float* aux;
     void* out;
     void* out2;
+    void* outT;       // optional (EPI_BIAS_GELU, EPI_DGELU): bf16 copy of out, transposed (N x M)
     int* err;
 };
 
@@ -118,13 +129,16 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     d |= (uint64_t)2 << 61;             // SWIZZLE_128B
     return d;
 }
-// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major, M = 128, N = TBN.
+template <int TBN>
+__host__ __device__ constexpr uint32_t idesc() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
-__device__ __forceinline__ void umma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t id, uint32_t acc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-        "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
+        "l"(da), "l"(db), "r"(id), "r"(acc));
 }
 __device__ __forceinline__ void umma_commit(uint64_t* b) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_u32(b)) : "memory");
@@ -151,15 +165,16 @@ __device__ __forceinline__ float dgelu(float z) {
 // ---------------------------------------------------------------------------
 // k_gemm
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, int TBN>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     k_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = s_u32(smem_raw);
-    GemmSmem& S = *reinterpret_cast<GemmSmem*>(smem_raw + (((raw + 1023u) & ~1023u) - raw));
+    GemmSmem<TBN>& S = *reinterpret_cast<GemmSmem<TBN>*>(smem_raw + (((raw + 1023u) & ~1023u) - raw));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int nk = (g.K + BK - 1) / BK;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * TBN;
+    const int kb = blockIdx.z * g.kchunks;                           // first K-chunk of this split
+    const int nk = min((g.K + BK - 1) / BK - kb, g.kchunks);         // >= 1: the host makes no empty split
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -172,7 +187,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&S.tmem_base)),
-                     "r"(BN));
+                     "r"(TBN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -188,9 +203,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                 S.abort = 1;
                 break;
             }
-            bar_expect(&S.full[s], TILE_A + TILE_B);
-            tma_load_2d(S.a[s], &ta, kc * BK, m0, &S.full[s]);
-            tma_load_2d(S.b[s], &tb, kc * BK, n0, &S.full[s]);
+            bar_expect(&S.full[s], TILE_A + tile_b<TBN>());
+            tma_load_2d(S.a[s], &ta, (kb + kc) * BK, m0, &S.full[s]);
+            tma_load_2d(S.b[s], &tb, (kb + kc) * BK, n0, &S.full[s]);
             issued = kc + 1;
         }
     } else if (warp == 1 && lane == 0) {
@@ -203,7 +218,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             tc_fence_after();
             const uint64_t da = sw128_desc(s_u32(S.a[s])), db = sw128_desc(s_u32(S.b[s]));
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk) umma(tmem, da + 2 * kk, db + 2 * kk, (kc | kk) != 0);
+            for (int kk = 0; kk < BK / 16; ++kk) umma(tmem, da + 2 * kk, db + 2 * kk, idesc<TBN>(), (kc | kk) != 0);
             umma_commit(&S.empty[s]);
         }
         umma_commit(&S.done);  // arrives once every MMA issued above has completed
@@ -212,17 +227,18 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
     const bool ok = __all_sync(0xffffffffu, bar_wait(&S.done, 0));
     tc_fence_after();
-    const int r = m0 + warp * 32 + lane;
+    const int quarter = warp & 3;
+    const int r = m0 + quarter * 32 + lane;
     if (ok) {
-        for (int c0 = 0; c0 < BN && n0 + c0 < g.N; c0 += 32) {
+        for (int c0 = (warp >> 2) * 32; c0 < TBN && n0 + c0 < g.N; c0 += 32 * EPI_GROUPS) {
             uint32_t v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
             if (r < g.M) {
                 const int nb = n0 + c0;
                 const int nv = min(32, g.N - nb);  // multiple of 8 (N % 8 == 0)
                 const size_t row = (size_t)r * g.N + nb;
                 if (MODE == EPI_F32 || MODE == EPI_BIAS_F32) {
-                    float* o = reinterpret_cast<float*>(g.out) + row;
+                    float* o = reinterpret_cast<float*>(g.out) + (size_t)blockIdx.z * g.zstride + row;
                     for (int j = 0; j < nv; j += 4) {
                         float4 q;
                         q.x = __uint_as_float(v[j]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j) : 0.f);
@@ -256,6 +272,22 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 #pragma unroll
                         for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(y[2 * t], y[2 * t + 1]);
                         *reinterpret_cast<uint4*>(o + j) = *reinterpret_cast<const uint4*>(h);
+                        if (g.outT) {
+                            // Transposed copy, rows r and r^1 (lanes l and l^1, both < M as M is even)
+                            // packed per column: the even lane stores column c, the odd lane c + 1.
+                            uint16_t* ot = reinterpret_cast<uint16_t*>(g.outT);
+                            const unsigned live = __activemask();
+#pragma unroll
+                            for (int t = 0; t < 4; ++t) {
+                                const uint32_t w = *reinterpret_cast<const uint32_t*>(&h[t]);
+                                const uint32_t other = __shfl_xor_sync(live, (lane & 1) ? (w & 0xffffu) : (w >> 16), 1);
+                                const size_t c = (size_t)(nb + j + 2 * t);
+                                if (lane & 1)
+                                    *reinterpret_cast<uint32_t*>(ot + (c + 1) * g.M + r - 1) = other | (w & 0xffff0000u);
+                                else
+                                    *reinterpret_cast<uint32_t*>(ot + c * g.M + r) = (w & 0xffffu) | (other << 16);
+                            }
+                        }
                     }
                 }
             }
@@ -270,7 +302,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TBN));
     }
 }
 
@@ -293,14 +325,43 @@ __global__ void k_transpose(int rows, int cols, const uint16_t* __restrict__ in,
     }
 }
 
-// out[n] += sum over the rows of in[r][n] (bf16 in, fp32 out, zeroed by the caller).
-__global__ void k_colsum(int rows, int cols, const __nv_bfloat16* __restrict__ in, float* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
-    const int r0 = blockIdx.y * 256, r1 = min(rows, r0 + 256);
+// out[i] = part[0][i] + part[1][i] + ... in that order: the FP32 partial products of a K-split GEMM
+// (n a multiple of 4; the order is fixed, so the sum is the same on every run).
+__global__ void k_sum_splits(int64_t n4, int splits, const float4* __restrict__ part, float4* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 s = __ldcs(part + i);
+        for (int z = 1; z < splits; ++z) {
+            const float4 t = __ldcs(part + (int64_t)z * n4 + i);
+            s.x += t.x; s.y += t.y; s.z += t.z; s.w += t.w;
+        }
+        out[i] = s;
+    }
+}
+
+// out[r] = sum over the columns of in[r][c] (bf16 in, fp32 out; cols a multiple of 8): one 256-thread
+// block per row, 16-byte loads, a fixed summation order.
+__global__ void __launch_bounds__(256) k_rowsum(int cols, const __nv_bfloat16* __restrict__ in, float* __restrict__ out) {
+    __shared__ float red[8];
+    const uint4* row = reinterpret_cast<const uint4*>(in + (size_t)blockIdx.x * cols);
     float s = 0.f;
-    for (int r = r0; r < r1; ++r) s += __bfloat162float(in[(size_t)r * cols + c]);
-    atomicAdd(out + c, s);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < cols / 8; c += 256) {
+        const uint4 q = __ldg(row + c);
+        const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&q);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float2 f = __bfloat1622float2(b[t]);
+            s += f.x + f.y;
+        }
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        out[blockIdx.x] = t;
+    }
 }
 
 // Input rows (fp32, n_in wide) -> bf16 rows padded with zeros to ld columns.
@@ -591,12 +652,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Tensor map of a row-major bf16 matrix (rows x cols), boxes of 64 columns x 128 rows, 128-byte swizzle.
-CUtensorMap bf16_map(const void* ptr, int64_t rows, int64_t cols) {
+CUtensorMap bf16_map(const void* ptr, int64_t rows, int64_t cols, uint32_t box_rows) {
     if (((uintptr_t)ptr & 15) || (cols % 8)) throw Fail(LCB_ERR_INVALID, "GEMM operand: 16-byte alignment and cols % 8 == 0 required");
     CUtensorMap m;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)BK, 128u};
+    cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -605,29 +666,50 @@ CUtensorMap bf16_map(const void* ptr, int64_t rows, int64_t cols) {
     return m;
 }
 
-constexpr size_t kGemmSmem = sizeof(GemmSmem) + 1024;
+template <int TBN>
+constexpr size_t gemm_smem() { return sizeof(GemmSmem<TBN>) + 1024; }
 
-template <int MODE>
+template <int MODE, int TBN>
 void launch_gemm_mode(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, cudaStream_t s) {
-    static cudaError_t attr = cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    static cudaError_t attr =
+        cudaFuncSetAttribute(k_gemm<MODE, TBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<TBN>());
     CK(attr);
-    dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN);
-    k_gemm<MODE><<<grid, GEMM_THREADS, kGemmSmem, s>>>(ta, tb, g);
+    dim3 grid((g.M + BM - 1) / BM, (g.N + TBN - 1) / TBN, (unsigned)(((g.K + BK - 1) / BK + g.kchunks - 1) / g.kchunks));
+    k_gemm<MODE, TBN><<<grid, GEMM_THREADS, gemm_smem<TBN>(), s>>>(ta, tb, g);
     CK(cudaGetLastError());
 }
 
 // Sets the dynamic shared-memory limit of every GEMM variant (needed before a
 // stream capture, during which the first launch of a variant cannot set it).
 void prepare_gemm_attributes() {
-    CK(cudaFuncSetAttribute(k_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-    CK(cudaFuncSetAttribute(k_gemm<EPI_BIAS_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-    CK(cudaFuncSetAttribute(k_gemm<EPI_BIAS_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-    CK(cudaFuncSetAttribute(k_gemm<EPI_DGELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+#define LCB_SMEM_ATTR(M, T) \
+    CK(cudaFuncSetAttribute(k_gemm<M, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<T>()))
+    LCB_SMEM_ATTR(EPI_F32, 128); LCB_SMEM_ATTR(EPI_BIAS_GELU, 128); LCB_SMEM_ATTR(EPI_BIAS_F32, 128);
+    LCB_SMEM_ATTR(EPI_DGELU, 128);
+    LCB_SMEM_ATTR(EPI_F32, 256); LCB_SMEM_ATTR(EPI_BIAS_GELU, 256); LCB_SMEM_ATTR(EPI_BIAS_F32, 256);
+    LCB_SMEM_ATTR(EPI_DGELU, 256);
+#undef LCB_SMEM_ATTR
 }
 
+int tile_n(int64_t N) { return N >= 256 ? 256 : 128; }  // 128 x 256 tiles where N allows
+
+// Number of K-splits for an FP32-output GEMM: enough CTAs to cover `sms` SMs, none of them empty.
+int split_count(int64_t M, int64_t N, int64_t K, int sms) {
+    const int64_t tiles = ((M + BM - 1) / BM) * ((N + tile_n(N) - 1) / tile_n(N)), nk = (K + BK - 1) / BK;
+    const int64_t s = std::max<int64_t>(1, std::min<int64_t>(sms / tiles, nk)), kc = (nk + s - 1) / s;
+    return (int)((nk + kc - 1) / kc);
+}
+
+// Upper bound of split_count(M, N, K, sms) over every K.
+int max_split_count(int64_t M, int64_t N, int sms) {
+    const int64_t tiles = ((M + BM - 1) / BM) * ((N + tile_n(N) - 1) / tile_n(N));
+    return (int)std::max<int64_t>(1, sms / tiles);
+}
+
+// splits > 1 (EPI_F32 only): split z writes its partial product to out + z * M * N.
 void gemm(int mode, int64_t M, int64_t N, int64_t K, const void* A, const void* B, const float* bias, const float* aux,
-          void* out, void* out2, int* err, cudaStream_t s) {
-    if (M <= 0 || N <= 0 || K <= 0 || N % 8 || K % 8 || M > INT32_MAX || N > 65535 * (int64_t)BN)
+          void* out, void* out2, int* err, cudaStream_t s, int splits = 1, void* outT = nullptr) {
+    if (M <= 0 || N <= 0 || K <= 0 || N % 8 || K % 8 || M > INT32_MAX || N > 65535 * (int64_t)128)
         throw Fail(LCB_ERR_INVALID, "GEMM sizes: M, N, K > 0 and N, K multiples of 8 required");
     if (((uintptr_t)out & 15) || (out2 && ((uintptr_t)out2 & 15)) || (aux && ((uintptr_t)aux & 15)))
         throw Fail(LCB_ERR_INVALID, "GEMM outputs must be 16-byte aligned");
@@ -635,15 +717,32 @@ void gemm(int mode, int64_t M, int64_t N, int64_t K, const void* A, const void* 
     if (mode == EPI_BIAS_GELU && !out2) throw Fail(LCB_ERR_INVALID, "pre-activation output required");
     if (mode == EPI_DGELU && !aux) throw Fail(LCB_ERR_INVALID, "pre-activation input required");
     if (!err) throw Fail(LCB_ERR_INVALID, "error word required");
-    const CUtensorMap ta = bf16_map(A, M, K), tb = bf16_map(B, N, K);
-    GemmArgs g{(int)M, (int)N, (int)K, bias, aux, out, out2, err};
-    switch (mode) {
-        case EPI_F32: launch_gemm_mode<EPI_F32>(ta, tb, g, s); break;
-        case EPI_BIAS_GELU: launch_gemm_mode<EPI_BIAS_GELU>(ta, tb, g, s); break;
-        case EPI_BIAS_F32: launch_gemm_mode<EPI_BIAS_F32>(ta, tb, g, s); break;
-        case EPI_DGELU: launch_gemm_mode<EPI_DGELU>(ta, tb, g, s); break;
+    if (outT && ((mode != EPI_BIAS_GELU && mode != EPI_DGELU) || M % 2 || ((uintptr_t)outT & 3)))
+        throw Fail(LCB_ERR_INVALID, "transposed copy: bf16 modes, even M, 4-byte aligned");
+    const int nk = (int)((K + BK - 1) / BK), kchunks = (nk + splits - 1) / std::max(splits, 1);
+    if (splits < 1 || (splits > 1 && mode != EPI_F32) || (nk + kchunks - 1) / kchunks != splits)
+        throw Fail(LCB_ERR_INVALID, "GEMM K-split must be an FP32-output split with no empty part");
+    const bool wide = tile_n(N) == 256;
+    const CUtensorMap ta = bf16_map(A, M, K, 128u), tb = bf16_map(B, N, K, wide ? 256u : 128u);
+    GemmArgs g{(int)M, (int)N, (int)K, kchunks, M * N, bias, aux, out, out2, outT, err};
+    switch (mode * 2 + (wide ? 1 : 0)) {
+        case EPI_F32 * 2: launch_gemm_mode<EPI_F32, 128>(ta, tb, g, s); break;
+        case EPI_F32 * 2 + 1: launch_gemm_mode<EPI_F32, 256>(ta, tb, g, s); break;
+        case EPI_BIAS_GELU * 2: launch_gemm_mode<EPI_BIAS_GELU, 128>(ta, tb, g, s); break;
+        case EPI_BIAS_GELU * 2 + 1: launch_gemm_mode<EPI_BIAS_GELU, 256>(ta, tb, g, s); break;
+        case EPI_BIAS_F32 * 2: launch_gemm_mode<EPI_BIAS_F32, 128>(ta, tb, g, s); break;
+        case EPI_BIAS_F32 * 2 + 1: launch_gemm_mode<EPI_BIAS_F32, 256>(ta, tb, g, s); break;
+        case EPI_DGELU * 2: launch_gemm_mode<EPI_DGELU, 128>(ta, tb, g, s); break;
+        case EPI_DGELU * 2 + 1: launch_gemm_mode<EPI_DGELU, 256>(ta, tb, g, s); break;
         default: throw Fail(LCB_ERR_INVALID, "unknown GEMM epilogue mode");
     }
+}
+
+void sum_splits(int64_t n, int splits, const float* part, float* out, cudaStream_t s) {
+    const int64_t n4 = n / 4;
+    k_sum_splits<<<(unsigned)std::min<int64_t>((n4 + 255) / 256, 1184), 256, 0, s>>>(
+        n4, splits, reinterpret_cast<const float4*>(part), reinterpret_cast<float4*>(out));
+    CK(cudaGetLastError());
 }
 
 void transpose(int64_t rows, int64_t cols, const void* in, void* out, cudaStream_t s) {
@@ -673,6 +772,7 @@ struct lcb_mlp {
     int device = 0;
     int n_in = 0, width = 0, n_hidden = 0, n_out = 0, nl = 0;
     int64_t max_batch = 0;
+    int sms = 0;                      // SM count (sizes the K-splits of the weight-gradient GEMMs)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<int> out, in;         // per layer (in padded to a multiple of 8)
@@ -683,8 +783,10 @@ struct lcb_mlp {
     DBuf<__nv_bfloat16> x0;           // packed input
     std::vector<DBuf<__nv_bfloat16>> y;  // hidden activations (bf16)
     std::vector<DBuf<float>> z;          // hidden pre-activations (fp32)
+    std::vector<DBuf<__nv_bfloat16>> yT; // hidden activations transposed (training only)
     DBuf<float> pred;
     DBuf<__nv_bfloat16> dz[2], dzt, xt;
+    DBuf<float> wsplit;               // FP32 partial products of the K-split weight-gradient GEMMs
     DBuf<int> err;
     DBuf<double> loss;
     DBuf<float> sub_x;                   // sub-chain: network inputs
@@ -705,6 +807,7 @@ struct lcb_mlp {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
         p.free(); m.free(); v.free(); g.free(); wbf.free(); wtbf.free(); x0.free(); pred.free(); dzt.free(); xt.free();
+        wsplit.free();
         dz[0].free(); dz[1].free(); err.free(); loss.free();
         sub_x.free(); sub_yp.free(); sub_lz.free(); sub_chi.free(); sub_lq.free(); sub_lqp.free(); sub_kde.free();
         sub_y.free(); sub_ls.free(); sub_comp.free(); sub_rnd.free();
@@ -712,6 +815,7 @@ struct lcb_mlp {
         sub_graph = nullptr;
         for (auto& t : y) t.free();
         for (auto& t : z) t.free();
+        for (auto& t : yT) t.free();
         if (own_stream && stream) cudaStreamDestroy(stream);
         stream = nullptr;
     }
@@ -723,7 +827,8 @@ struct lcb_mlp {
         if (h) throw Fail(LCB_ERR_DEVICE_CHECK, "a bounded wait in the surrogate GEMM timed out");
     }
 
-    void forward(const float* x, int64_t B, float* y_out) {
+    // keep_t: also store each hidden activation transposed (yT), for the weight gradients
+    void forward(const float* x, int64_t B, float* y_out, bool keep_t = false) {
         if (B <= 0 || B > max_batch) throw Fail(LCB_ERR_INVALID, "batch size out of range");
         const int64_t nx = B * in[0];
         k_pack_input<<<(unsigned)((nx + 255) / 256), 256, 0, stream>>>((int)B, n_in, in[0], x, x0.p);
@@ -731,7 +836,8 @@ struct lcb_mlp {
         const void* a = x0.p;
         for (int l = 0; l < nl; ++l) {
             if (l + 1 < nl) {
-                gemm(EPI_BIAS_GELU, B, out[l], in[l], a, wbf.p + tab.wbf[l], b(l), nullptr, y[l].p, z[l].p, err.p, stream);
+                gemm(EPI_BIAS_GELU, B, out[l], in[l], a, wbf.p + tab.wbf[l], b(l), nullptr, y[l].p, z[l].p, err.p, stream,
+                     1, keep_t ? yT[l].p : nullptr);
                 a = y[l].p;
             } else {
                 gemm(EPI_BIAS_F32, B, out[l], in[l], a, wbf.p + tab.wbf[l], b(l), nullptr, y_out ? y_out : pred.p,
@@ -742,24 +848,34 @@ struct lcb_mlp {
 
     void backward(const float* x, const float* target, int64_t B) {
         if (B % 8) throw Fail(LCB_ERR_INVALID, "training batch must be a multiple of 8");
-        forward(x, B, nullptr);
+        forward(x, B, nullptr, true);
         const int64_t npred = B * n_out;
         CK(cudaMemsetAsync(g.p, 0, nparam * sizeof(float), stream));
         k_mse_grad<<<(unsigned)std::min<int64_t>((npred + 255) / 256, 1184), 256, 0, stream>>>(
             npred, 1.0f / (float)npred, pred.p, target, dz[0].p, loss.p);
         CK(cudaGetLastError());
+        // dzt holds the current layer's output gradient transposed: made here for the last layer, then by
+        // the dGELU GEMM that produces each earlier layer's gradient
+        transpose(B, n_out, dz[0].p, dzt.p, stream);
         int cur = 0;
         for (int l = nl - 1; l >= 0; --l) {
-            const void* xl = l == 0 ? (const void*)x0.p : (const void*)y[l - 1].p;
-            transpose(B, out[l], dz[cur].p, dzt.p, stream);
-            transpose(B, in[l], xl, xt.p, stream);
-            gemm(EPI_F32, out[l], in[l], B, dzt.p, xt.p, nullptr, nullptr, gW(l), nullptr, err.p, stream);
-            dim3 cg((unsigned)((out[l] + 127) / 128), (unsigned)((B + 255) / 256));
-            k_colsum<<<cg, 128, 0, stream>>>((int)B, out[l], dz[cur].p, gb(l));
+            const void* xlt = l > 0 ? (const void*)yT[l - 1].p : (const void*)xt.p;
+            if (l == 0) transpose(B, in[0], x0.p, xt.p, stream);
+            // dW = dz^T x: K = batch is long and the output small, so K is split across the SMs
+            const int ns = split_count(out[l], in[l], B, sms);
+            if (ns > 1) {
+                if ((int64_t)ns * out[l] * in[l] > (int64_t)wsplit.n) throw Fail(LCB_ERR_INVALID, "weight-gradient split workspace too small");
+                gemm(EPI_F32, out[l], in[l], B, dzt.p, xlt, nullptr, nullptr, wsplit.p, nullptr, err.p, stream, ns);
+                sum_splits((int64_t)out[l] * in[l], ns, wsplit.p, gW(l), stream);
+            } else {
+                gemm(EPI_F32, out[l], in[l], B, dzt.p, xlt, nullptr, nullptr, gW(l), nullptr, err.p, stream);
+            }
+            // db = row sums of dz^T
+            k_rowsum<<<(unsigned)out[l], 256, 0, stream>>>((int)B, dzt.p, gb(l));
             CK(cudaGetLastError());
-            if (l > 0) {
+            if (l > 0) {  // stream order: the GEMMs above have read dzt before this one rewrites it
                 gemm(EPI_DGELU, B, in[l], out[l], dz[cur].p, wtbf.p + tab.wbf[l], nullptr, z[l - 1].p, dz[cur ^ 1].p,
-                     nullptr, err.p, stream);
+                     nullptr, err.p, stream, 1, dzt.p);
                 cur ^= 1;
             }
         }
@@ -799,6 +915,7 @@ int lcb_mlp_create(int device, int n_in, int width, int n_hidden, int n_out, int
         CK(cudaGetDeviceProperties(&prop, device));
         if (prop.major < 10) throw Fail(LCB_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
         N->n_in = n_in; N->width = width; N->n_hidden = n_hidden; N->n_out = n_out;
+        N->sms = prop.multiProcessorCount;
         N->nl = n_hidden + 1;
         N->max_batch = (max_batch + 7) / 8 * 8;
         for (int l = 0; l < N->nl; ++l) {
@@ -827,16 +944,22 @@ int lcb_mlp_create(int device, int n_in, int width, int n_hidden, int n_out, int
         N->x0.alloc(B * N->in[0]);
         N->y.resize(N->nl - 1);
         N->z.resize(N->nl - 1);
+        N->yT.resize(N->nl - 1);
         for (int l = 0; l + 1 < N->nl; ++l) {
             N->y[l].alloc(B * width);
             N->z[l].alloc(B * width);
+            N->yT[l].alloc(B * width);
         }
         const int wmax = std::max(width, n_out);
         N->pred.alloc(B * n_out);
         N->dz[0].alloc(B * wmax);
         N->dz[1].alloc(B * wmax);
         N->dzt.alloc(B * wmax);
-        N->xt.alloc(B * std::max(width, N->in[0]));
+        N->xt.alloc(B * N->in[0]);
+        int64_t nsplit = 0;
+        for (int l = 0; l < N->nl; ++l)
+            nsplit = std::max(nsplit, (int64_t)max_split_count(N->out[l], N->in[l], N->sms) * N->out[l] * N->in[l]);
+        N->wsplit.alloc(nsplit);
         N->err.alloc(1);
         N->loss.alloc(1);
         N->sub_x.alloc(B * N->in[0]);
