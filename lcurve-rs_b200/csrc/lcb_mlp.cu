@@ -73,6 +73,8 @@ struct GemmSmem {
     uint32_t tmem_base;
     int abort;
 };
+// the epilogue's per-warp staging (6 KB a warp) reuses a[] and b[]
+static_assert((GEMM_THREADS / 32) * 6144 <= STAGES * (TILE_A + tile_b<128>()), "epilogue staging");
 
 struct GemmArgs {
     int M, N, K;
@@ -228,60 +230,75 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     const bool ok = __all_sync(0xffffffffu, bar_wait(&S.done, 0));
     tc_fence_after();
     const int quarter = warp & 3;
-    const int r = m0 + quarter * 32 + lane;
-    if (ok) {
+    const int rbase = m0 + quarter * 32;          // first output row of this warp's TMEM lanes
+    const int rows = min(32, g.M - rbase);        // rows in range (even when M is)
+    // Per-warp staging, 32 rows x 32 columns as FP32 (4 KB) and as BF16 (2 KB), in the operand
+    // buffers (idle once S.done has fired: every copy has landed and every MMA has read it).
+    // 16-byte chunks are XOR-swizzled by row so the row-per-lane accesses (TMEM layout) and the
+    // row-contiguous accesses of the global copies both spread over all banks.
+    uint8_t* stage = &S.a[0][0] + warp * 6144;
+    float* stf = reinterpret_cast<float*>(stage);
+    uint8_t* stb = stage + 4096;
+    auto f32_at = [&](int i, int c) { return reinterpret_cast<float4*>(stf + i * 32 + ((c ^ (i & 7)) << 2)); };
+    auto b16_at = [&](int i, int c) { return reinterpret_cast<uint4*>(stb + i * 64 + ((c ^ ((i >> 1) & 3)) << 4)); };
+    if (ok && rows > 0) {
         for (int c0 = (warp >> 2) * 32; c0 < TBN && n0 + c0 < g.N; c0 += 32 * EPI_GROUPS) {
             uint32_t v[32];
             tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
-            if (r < g.M) {
-                const int nb = n0 + c0;
-                const int nv = min(32, g.N - nb);  // multiple of 8 (N % 8 == 0)
-                const size_t row = (size_t)r * g.N + nb;
-                if (MODE == EPI_F32 || MODE == EPI_BIAS_F32) {
-                    float* o = reinterpret_cast<float*>(g.out) + (size_t)blockIdx.z * g.zstride + row;
-                    for (int j = 0; j < nv; j += 4) {
-                        float4 q;
-                        q.x = __uint_as_float(v[j]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j) : 0.f);
-                        q.y = __uint_as_float(v[j + 1]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 1) : 0.f);
-                        q.z = __uint_as_float(v[j + 2]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 2) : 0.f);
-                        q.w = __uint_as_float(v[j + 3]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 3) : 0.f);
-                        *reinterpret_cast<float4*>(o + j) = q;
-                    }
-                } else {
-                    __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(g.out) + row;
-                    for (int j = 0; j < nv; j += 8) {
-                        float y[8];
-                        if (MODE == EPI_BIAS_GELU) {
-                            float z[8];
+            const int nb = n0 + c0;
+            const int nv = min(32, g.N - nb);  // multiple of 8 (N % 8 == 0)
+            if (MODE == EPI_DGELU) {  // pre-activations in, row-contiguous
 #pragma unroll
-                            for (int t = 0; t < 8; ++t) {
-                                z[t] = __uint_as_float(v[j + t]) + __ldg(g.bias + nb + j + t);
-                                y[t] = gelu(z[t]);
-                            }
-                            float* o2 = reinterpret_cast<float*>(g.out2) + row + j;
-                            *reinterpret_cast<float4*>(o2) = make_float4(z[0], z[1], z[2], z[3]);
-                            *reinterpret_cast<float4*>(o2 + 4) = make_float4(z[4], z[5], z[6], z[7]);
-                        } else {  // EPI_DGELU
-                            const float4 a0 = __ldg(reinterpret_cast<const float4*>(g.aux + row + j));
-                            const float4 a1 = __ldg(reinterpret_cast<const float4*>(g.aux + row + j + 4));
-                            const float zz[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+                for (int k = 0; k < 8; ++k) {
+                    const int i = k * 4 + (lane >> 3), c = lane & 7;
+                    if (i < rows && c * 4 < nv)
+                        *f32_at(i, c) = __ldg(reinterpret_cast<const float4*>(g.aux + (size_t)(rbase + i) * g.N + nb + c * 4));
+                }
+                __syncwarp();
+            }
+            // lane = row: epilogue arithmetic into the staging tiles
+            if (MODE == EPI_F32 || MODE == EPI_BIAS_F32) {
+                for (int j = 0; j < nv; j += 4) {
+                    float4 q;
+                    q.x = __uint_as_float(v[j]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j) : 0.f);
+                    q.y = __uint_as_float(v[j + 1]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 1) : 0.f);
+                    q.z = __uint_as_float(v[j + 2]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 2) : 0.f);
+                    q.w = __uint_as_float(v[j + 3]) + (MODE == EPI_BIAS_F32 ? __ldg(g.bias + nb + j + 3) : 0.f);
+                    *f32_at(lane, j >> 2) = q;
+                }
+            } else {
+                for (int j = 0; j < nv; j += 8) {
+                    float y[8];
+                    if (MODE == EPI_BIAS_GELU) {
+                        float z[8];
 #pragma unroll
-                            for (int t = 0; t < 8; ++t) y[t] = __uint_as_float(v[j + t]) * dgelu(zz[t]);
+                        for (int t = 0; t < 8; ++t) {
+                            z[t] = __uint_as_float(v[j + t]) + __ldg(g.bias + nb + j + t);
+                            y[t] = gelu(z[t]);
                         }
-                        __align__(16) __nv_bfloat162 h[4];
+                        *f32_at(lane, j >> 2) = make_float4(z[0], z[1], z[2], z[3]);
+                        *f32_at(lane, (j >> 2) + 1) = make_float4(z[4], z[5], z[6], z[7]);
+                    } else {  // EPI_DGELU
+                        const float4 a0 = *f32_at(lane, j >> 2), a1 = *f32_at(lane, (j >> 2) + 1);
+                        const float zz[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
-                        for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(y[2 * t], y[2 * t + 1]);
-                        *reinterpret_cast<uint4*>(o + j) = *reinterpret_cast<const uint4*>(h);
-                        if (g.outT) {
-                            // Transposed copy, rows r and r^1 (lanes l and l^1, both < M as M is even)
-                            // packed per column: the even lane stores column c, the odd lane c + 1.
-                            uint16_t* ot = reinterpret_cast<uint16_t*>(g.outT);
-                            const unsigned live = __activemask();
+                        for (int t = 0; t < 8; ++t) y[t] = __uint_as_float(v[j + t]) * dgelu(zz[t]);
+                    }
+                    __align__(16) __nv_bfloat162 h[4];
 #pragma unroll
-                            for (int t = 0; t < 4; ++t) {
-                                const uint32_t w = *reinterpret_cast<const uint32_t*>(&h[t]);
-                                const uint32_t other = __shfl_xor_sync(live, (lane & 1) ? (w & 0xffffu) : (w >> 16), 1);
-                                const size_t c = (size_t)(nb + j + 2 * t);
+                    for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(y[2 * t], y[2 * t + 1]);
+                    *b16_at(lane, j >> 3) = *reinterpret_cast<const uint4*>(h);
+                    if (g.outT) {
+                        // Transposed copy: rows r and r^1 (lanes l and l^1; rows is even) packed per
+                        // column, the even lane storing column c and the odd lane column c + 1.
+                        uint16_t* ot = reinterpret_cast<uint16_t*>(g.outT);
+                        const int r = rbase + lane;
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            const uint32_t w = *reinterpret_cast<const uint32_t*>(&h[t]);
+                            const uint32_t other = __shfl_xor_sync(0xffffffffu, (lane & 1) ? (w & 0xffffu) : (w >> 16), 1);
+                            const size_t c = (size_t)(nb + j + 2 * t);
+                            if (lane < rows) {
                                 if (lane & 1)
                                     *reinterpret_cast<uint32_t*>(ot + (c + 1) * g.M + r - 1) = other | (w & 0xffff0000u);
                                 else
@@ -291,6 +308,28 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                     }
                 }
             }
+            __syncwarp();
+            // staging -> global, row-contiguous (8 lanes per 128-byte FP32 row, 4 per 64-byte BF16 row)
+            if (MODE != EPI_DGELU) {
+                float* dst = MODE == EPI_BIAS_GELU ? reinterpret_cast<float*>(g.out2)
+                                                   : reinterpret_cast<float*>(g.out) + (size_t)blockIdx.z * g.zstride;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int i = k * 4 + (lane >> 3), c = lane & 7;
+                    if (i < rows && c * 4 < nv)
+                        *reinterpret_cast<float4*>(dst + (size_t)(rbase + i) * g.N + nb + c * 4) = *f32_at(i, c);
+                }
+            }
+            if (MODE == EPI_BIAS_GELU || MODE == EPI_DGELU) {
+                __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(g.out);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int i = k * 8 + (lane >> 2), c = lane & 3;
+                    if (i < rows && c * 8 < nv)
+                        *reinterpret_cast<uint4*>(dst + (size_t)(rbase + i) * g.N + nb + c * 8) = *b16_at(i, c);
+                }
+            }
+            __syncwarp();  // the staging tiles are rewritten by the next chunk
         }
     }
     tc_fence_before();
