@@ -98,6 +98,7 @@ struct lcb_batch {
     std::vector<lcb_datum> data;
     std::vector<int64_t> start, count;
     lcb::Plan plan;
+    lcb::Plan spare;  // the plan before the last lcb_batch_set_params: its storage is planned into next
     DeviceSet dev;
     cudaGraphExec_t graph = nullptr;
     int graph_scale = -1;
@@ -620,10 +621,12 @@ int lcb_batch_set_params(lcb_batch* B, const char* const* names, int ndim, const
         }
         std::vector<const lcb::Model*> mp(n);
         for (int64_t i = 0; i < n; ++i) mp[i] = &B->models[i];
-        lcb::Plan P;
+        // plan into the previous call's storage (kept capacity: no allocation or first-touch page
+        // faults when a resident batch is re-parameterised step after step)
+        lcb::Plan& P = B->spare;
         lcb::plan_batch(mp.data(), n, B->data.data(), B->start.data(), B->count.data(), C->num_sms, P);
-        bool same = P.shape_key == B->plan.shape_key;
-        B->plan = std::move(P);
+        const bool same = P.shape_key == B->plan.shape_key;
+        std::swap(B->plan, P);
         // unchanged shapes: only the model table and the tables derived from it change
         upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
         if (!same && B->graph) {
