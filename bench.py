@@ -21,6 +21,9 @@ data (lcurve-rs_b200/workloads.py).
           Defaults are a reduced run (524k curves, 3000 steps); --mcmc-full
           runs the full 1M-curve, 20000-step configuration.
 
+  --train-profile K : only the surrogate's training step (8192 curves), K
+          steps after --warmup, one JSON line (the profiling entry point).
+
 Multi-GPU (torchrun): weak scaling, each rank evaluates its own 1024-model
 batch (seed 1234 + rank); no collective on the data path, only the timing
 reduction.  `--impl reference` times the CPU oracle (the FP64 restatement of
@@ -29,6 +32,7 @@ the reference's Rayon path) on the host cores instead.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib
 import json
 import os
@@ -68,6 +72,8 @@ def parse():
     p.add_argument("--mcmc-burn", type=int, default=500)
     p.add_argument("--mcmc-substeps", type=int, default=2)
     p.add_argument("--mcmc-bandwidth", type=float, default=0.6, help="KDE bandwidth in units of Scott's factor")
+    p.add_argument("--train-profile", type=int, default=0, metavar="K",
+                   help="time K surrogate training steps (8192 curves) alone, print one JSON line and exit")
     a = p.parse_args()
     if a.mcmc_full:
         a.mcmc_curves, a.mcmc_epochs, a.mcmc_steps = 1048576, 300, 20000
@@ -221,6 +227,40 @@ def weak_value(world: int, models_per_rank: int, ms_max: float) -> float:
     return world * models_per_rank / (ms_max / 1e3)
 
 
+def run_train_profile(args, lcb):
+    """K training steps of the surrogate network (5 -> 4 x 512 -> 256, 8192
+    curves a step: forward, backward, Adam) on seeded synthetic inputs, after
+    --warmup steps; host wall clock around the stream (one sync each side).
+    The launch-list profile of the surrogate's kernels runs this."""
+    import torch
+
+    S = importlib.import_module("lcurve-rs_b200.surrogate")
+    sur = S.Surrogate()
+    b = sur.max_batch
+    g = torch.Generator(device=sur.dev).manual_seed(0)
+    x = torch.rand(b, len(S.PARAMS), device=sur.dev, generator=g) * 2 - 1
+    y = torch.randn(b, sur.n_phase, device=sur.dev, generator=g)
+    torch.cuda.synchronize()
+
+    def step():
+        lcb._capi.check_mlp(sur.L.lcb_mlp_train_step(sur._h, ctypes.c_void_p(x.data_ptr()),
+                                                     ctypes.c_void_p(y.data_ptr()), b, 1e-3, 0.9, 0.999, 1e-8, 0.0))
+
+    for _ in range(args.warmup):
+        step()
+    lcb._capi.check_mlp(sur.L.lcb_mlp_sync(sur._h))
+    t0 = time.perf_counter()
+    for _ in range(args.train_profile):
+        step()
+    lcb._capi.check_mlp(sur.L.lcb_mlp_sync(sur._h))
+    dt = (time.perf_counter() - t0) / max(args.train_profile, 1)
+    n_par = len(S.PARAMS)
+    flops = 6 * b * ((n_par + 7) // 8 * 8 * sur.width + (sur.n_hidden - 1) * sur.width ** 2 + sur.width * sur.n_phase)
+    print(json.dumps({"surrogate_train_step_ms": dt * 1e3, "batch": b, "steps": args.train_profile,
+                      "warmup": args.warmup, "gemm_tflops_6bp": flops / dt / 1e12,
+                      "network": f"{n_par} -> {sur.n_hidden} x {sur.width} (GELU) -> {sur.n_phase}"}))
+
+
 def run_mcmc(args, lcb):
     """Surrogate delayed-acceptance MCMC against plain engine MCMC: 256
     walkers on the fixed 256-phase problem (fiducial curve + 1% noise), all
@@ -307,6 +347,9 @@ def main():
     lcb = importlib.import_module("lcurve-rs_b200")
     W = importlib.import_module("lcurve-rs_b200.workloads")
     lcb.set_device(f"cuda:{local}")
+    if args.train_profile:
+        run_train_profile(args, lcb)
+        return
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     lcb.set_stream(stream.cuda_stream)  # the library's work and the timing events share this stream
