@@ -15,7 +15,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
-#include <functional>
+#include <mutex>
 #include <thread>
 
 namespace lcb {
@@ -131,8 +131,9 @@ double dlpdlt(double wave, double temp) {
 class BulirschStoer {  // bsstep.rs:13-324
 public:
     static constexpr int kK = 8;
+    template <class F>  // F(y, dydx): the right-hand side, inlined
     void step(double* y, const double* dydx, double& x, double htry, double eps, double& hdid, double& hnext,
-              const std::function<void(const double*, double*)>& f) {
+              const F& f) {
         static const int nseq[kK + 1] = {2, 4, 6, 8, 10, 12, 14, 16, 18};
         const double safe1 = 0.25, safe2 = 0.7, redmax = 1.0e-5, redmin = 0.7, tiny = 1.0e-30, scalmx = 0.1;
         double err[kK] = {0}, ysav[6], yseq[6], yerr[6];
@@ -203,8 +204,9 @@ public:
     }
 
 private:
+    template <class F>
     static void midpoint(const double* y, const double* dydx, double htot, int n, double* yout,
-                         const std::function<void(const double*, double*)>& f) {  // bsstep.rs:57-93
+                         const F& f) {  // bsstep.rs:57-93
         double h = htot / n, ym[6], yn[6];
         for (int i = 0; i < 6; ++i) { ym[i] = y[i]; yn[i] = y[i] + h * dydx[i]; }
         f(yn, yout);
@@ -265,7 +267,7 @@ void stream_step(double q, double* y, double& t, double htry, BulirschStoer& bs,
 inline double radius3(const double* y) { return std::sqrt(sq(y[0]) + sq(y[1]) + sq(y[2])); }
 
 // strinit + stradv(q, r, v, rad, 1e-10, 1e-3) (stream.rs:8-20, 82-145).
-void stream_to_radius(double q, double rad, double out[3]) {
+void stream_to_radius_uncached(double q, double rad, double out[3]) {
     const double small = 1.0e-5;
     double rl1 = host_xl1(q), mu = q / (1.0 + q);
     double a = (1.0 - mu) / cube(rl1) + mu / cube(1.0 - rl1);
@@ -299,6 +301,33 @@ void stream_to_radius(double q, double rad, double out[3]) {
         }
         if (t > 10.0) throw model_err("stradv: took too long without crossing radius=" + std::to_string(rad));
     }
+}
+
+// stream_to_radius_uncached memoised on (q, rad), process-wide: the integration is ~20,000
+// serial right-hand-side evaluations (the reference's 1e-3 step cap), and fits, batches and
+// repeated light curves mostly revisit the same geometry.  The result is a function of (q, rad)
+// alone, so a hit returns exactly what the integration would; failures are not cached.
+void stream_to_radius(double q, double rad, double out[3]) {
+    struct Entry {
+        double q, rad, xyz[3];
+        bool used;
+    };
+    constexpr int kEntries = 64;
+    static std::mutex mu;
+    static Entry cache[kEntries] = {};
+    static int next = 0;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        for (const Entry& e : cache)
+            if (e.used && e.q == q && e.rad == rad) {
+                out[0] = e.xyz[0]; out[1] = e.xyz[1]; out[2] = e.xyz[2];
+                return;
+            }
+    }
+    stream_to_radius_uncached(q, rad, out);
+    std::lock_guard<std::mutex> g(mu);
+    cache[next] = Entry{q, rad, {out[0], out[1], out[2]}, true};
+    next = (next + 1) % kEntries;
 }
 
 // Latitude bands of one star grid (grid.rs:157-322) appended to `bands`;
