@@ -72,6 +72,12 @@ def test_trained_surrogate_gains_over_plain_mcmc(lcb, mods):
     eng = S.CurveEngine(setup, data=data)
     sur.bind_data(data)
     start = M.run_delayed(eng, sur, M.initial_walkers(256, S.TRUTH, seed=3), 300, seed=4, substeps=32).chain[-1]
+    # one-time costs outside the timed runs: a resident batch (and its captured graph) for every
+    # engine batch size, and the sub-chain graph of this move
+    for size in eng.sizes:
+        eng.chisq(start[:size])
+    M.run_plain(eng, start, 3, seed=6, move="kde", bandwidth=0.6)
+    M.run_delayed(eng, sur, start, 3, seed=6, substeps=2, move="kde", bandwidth=0.6)
     # same move (KDE proposals from the other half) with and without the surrogate screen, 256 walkers
     plain = M.run_plain(eng, start, 200, seed=5, move="kde", bandwidth=0.6)
     da = M.run_delayed(eng, sur, start, 200, seed=5, substeps=2, move="kde", bandwidth=0.6)
