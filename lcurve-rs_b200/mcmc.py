@@ -69,8 +69,9 @@ class KDE:
     which is what keeps the move valid with the complement held fixed."""
 
     comp: np.ndarray
-    chol: np.ndarray
-    prec: np.ndarray
+    chol: np.ndarray   # kernel covariance = chol chol^T
+    prec: np.ndarray   # its inverse
+    white: np.ndarray  # chol^-1: whitened differences white (y - c) have |.|^2 = (y-c)^T prec (y-c)
 
     @classmethod
     def of(cls, comp: np.ndarray, bandwidth: float = 1.0) -> "KDE":
@@ -79,11 +80,17 @@ class KDE:
         h2 = (bandwidth * m ** (-1.0 / (d + 4))) ** 2
         cov = np.cov(comp, rowvar=False) * h2
         cov = cov + np.diag(1e-12 * np.diag(cov) + 1e-300)
-        return cls(comp, np.linalg.cholesky(cov), np.linalg.inv(cov))
+        chol = np.linalg.cholesky(cov)
+        return cls(comp, chol, np.linalg.inv(cov), np.linalg.inv(chol))
 
     def logq(self, y: np.ndarray) -> np.ndarray:
-        diff = y[:, None, :] - self.comp[None, :, :]
-        e = -0.5 * np.einsum("nmi,ij,nmj->nm", diff, self.prec, diff)
+        # squared Mahalanobis distances |a - b|^2 = |a|^2 + |b|^2 - 2 a.b of whitened points, centred
+        # on the components' mean so the coordinates are O(1) and the expansion loses nothing
+        c0 = self.comp.mean(axis=0)
+        yw = (np.atleast_2d(y) - c0) @ self.white.T
+        cw = (self.comp - c0) @ self.white.T
+        d2 = np.einsum("ni,ni->n", yw, yw)[:, None] + np.einsum("mi,mi->m", cw, cw)[None, :] - 2.0 * (yw @ cw.T)
+        e = -0.5 * np.maximum(d2, 0.0)
         mx = e.max(axis=1, keepdims=True)
         return mx[:, 0] + np.log(np.exp(e - mx).sum(axis=1))
 
