@@ -55,6 +55,13 @@ int  lcb_mlp_backward(lcb_mlp* net, const float* x_dev, const float* target_dev,
 /* lcb_mlp_backward followed by one Adam step (decoupled weight decay). */
 int  lcb_mlp_train_step(lcb_mlp* net, const float* x_dev, const float* target_dev, int64_t batch, float lr,
                         float beta1, float beta2, float eps, float weight_decay);
+/* Data-parallel training, one network per GPU: the device buffer of n FP32
+ * gradients that lcb_mlp_backward writes (the lcb_mlp_get_params layout), to be
+ * reduced in place across ranks (e.g. an NCCL all-reduce averaging it, ordered
+ * on the network's stream), then lcb_mlp_adam_step applies it.  backward +
+ * adam_step with no reduction in between is exactly lcb_mlp_train_step. */
+int  lcb_mlp_grads_device(lcb_mlp* net, float** grads_dev, int64_t* n);
+int  lcb_mlp_adam_step(lcb_mlp* net, float lr, float beta1, float beta2, float eps, float weight_decay);
 /* Accumulated loss since the last call, then reset (synchronises). */
 int  lcb_mlp_take_loss(lcb_mlp* net, double* loss_sum);
 /* Waits for the network's stream; LCB_ERR_DEVICE_CHECK if a device wait timed out. */

@@ -49,8 +49,8 @@ SYMBOLS = [
     # surrogate (lcurve_b200_surrogate.h)
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
-    "lcb_mlp_train_step", "lcb_mlp_take_loss", "lcb_mlp_sync", "lcb_mlp_gemm", "lcb_logflux_chisq",
-    "lcb_surrogate_subchain",
+    "lcb_mlp_train_step", "lcb_mlp_grads_device", "lcb_mlp_adam_step", "lcb_mlp_take_loss", "lcb_mlp_sync",
+    "lcb_mlp_gemm", "lcb_logflux_chisq", "lcb_surrogate_subchain",
 ]
 
 _lib = None
@@ -106,6 +106,8 @@ def load():
         "lcb_mlp_forward": ([vp, vp, i64, vp], i),
         "lcb_mlp_backward": ([vp, vp, vp, i64], i),
         "lcb_mlp_train_step": ([vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float], i),
+        "lcb_mlp_grads_device": ([vp, C.POINTER(C.POINTER(C.c_float)), i64p], i),
+        "lcb_mlp_adam_step": ([vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float], i),
         "lcb_mlp_take_loss": ([vp, dp], i),
         "lcb_mlp_sync": ([vp], i),
         "lcb_mlp_gemm": ([i, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, vp], i),

@@ -1142,6 +1142,21 @@ int lcb_mlp_train_step(lcb_mlp* net, const float* x_dev, const float* target_dev
     });
 }
 
+int lcb_mlp_grads_device(lcb_mlp* net, float** grads_dev, int64_t* n) {
+    if (!net || !grads_dev || !n) return LCB_ERR_INVALID;
+    *grads_dev = net->g.p;
+    *n = net->nparam;
+    return LCB_OK;
+}
+
+int lcb_mlp_adam_step(lcb_mlp* net, float lr, float beta1, float beta2, float eps, float weight_decay) {
+    if (!net) return LCB_ERR_INVALID;
+    return guard([&] {
+        CK(cudaSetDevice(net->device));
+        net->adam(lr, beta1, beta2, eps, weight_decay);
+    });
+}
+
 int lcb_mlp_take_loss(lcb_mlp* net, double* loss_sum) {
     if (!net || !loss_sum) return LCB_ERR_INVALID;
     return guard([&] {

@@ -141,6 +141,13 @@ def generate_curves(setup: CurveSetup, theta: np.ndarray, chunk: int = 4096, log
     return out
 
 
+def shard_rows(k: int, batch: int, rank: int, world: int) -> slice:
+    """Rows of the k-th global batch (of `batch` rows, a multiple of `world`)
+    that data-parallel rank `rank` trains on: equal contiguous shards."""
+    local = batch // world
+    return slice(k * batch + rank * local, k * batch + (rank + 1) * local)
+
+
 def _shape(flux: np.ndarray) -> np.ndarray:
     lf = np.log(flux)
     return lf - lf.mean(axis=1, keepdims=True)
@@ -203,14 +210,26 @@ class Surrogate:
         return torch.as_tensor(x).to(self.dev)
 
     def fit(self, theta: np.ndarray, flux: np.ndarray, epochs: int = 60, batch: int = 8192, lr: float = 2e-3,
-            lr_min: float = 2e-5, log=None) -> list[float]:
+            lr_min: float = 2e-5, log=None, group=None) -> list[float]:
         """Trains on (theta, flux) rows with finite fluxes; cosine learning-rate
         schedule, Adam.  Returns the mean training loss of each epoch.
 
         The target is the curve's shape, ln f_j minus the curve's mean ln f:
         the likelihood it serves fits the flux scale per model (scale=True),
-        so the overall level carries no information and is not learned."""
+        so the overall level carries no information and is not learned.
+
+        group: a torch.distributed process group (one rank per GPU, every rank
+        with the same data, seed and arguments) for data-parallel training:
+        each global batch is split into equal contiguous shards, one per rank
+        (shard_rows), and the ranks' gradients are averaged by an all-reduce on
+        the network's stream before the Adam step, so every rank takes the
+        step of the whole batch and the weights stay identical.  The returned
+        losses are this rank's shards'."""
         torch = _torch()
+        rank, world = 0, 1
+        if group is not None:
+            import torch.distributed as dist  # noqa: PLC0415
+            rank, world = dist.get_rank(group), dist.get_world_size(group)
         ok = np.all(np.isfinite(flux), axis=1) & np.all(flux > 0, axis=1)
         theta, flux = theta[ok], flux[ok]
         with torch.cuda.stream(self._stream):
@@ -223,8 +242,13 @@ class Surrogate:
             X = self._x(theta)
         self._stream.synchronize()
         n = X.shape[0]
-        batch = min(batch, self.max_batch, n - n % 8)
+        local = min(batch // world, self.max_batch, (n // world) - (n // world) % 8)
+        local -= local % 8
+        if local <= 0:
+            raise ValueError("too few rows for one batch of 8 per rank")
+        batch = local * world
         steps_per_epoch = n // batch
+        grads = self._grads_tensor() if group is not None else None
         total = epochs * steps_per_epoch
         g = torch.Generator(device=self.dev).manual_seed(0)
         losses = []
@@ -236,12 +260,20 @@ class Surrogate:
             for k in range(steps_per_epoch):
                 rate = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * step / max(total, 1)))
                 with torch.cuda.stream(self._stream):
-                    idx = perm[k * batch:(k + 1) * batch]
+                    idx = perm[shard_rows(k, batch, rank, world)]
                     xb = X.index_select(0, idx)
                     yb = Y.index_select(0, idx)
-                _capi.check_mlp(self.L.lcb_mlp_train_step(self._h, C.c_void_p(xb.data_ptr()),
-                                                          C.c_void_p(yb.data_ptr()), batch, rate, 0.9, 0.999, 1e-8,
-                                                          0.0))
+                if group is None:
+                    _capi.check_mlp(self.L.lcb_mlp_train_step(self._h, C.c_void_p(xb.data_ptr()),
+                                                              C.c_void_p(yb.data_ptr()), local, rate, 0.9, 0.999,
+                                                              1e-8, 0.0))
+                else:
+                    _capi.check_mlp(self.L.lcb_mlp_backward(self._h, C.c_void_p(xb.data_ptr()),
+                                                            C.c_void_p(yb.data_ptr()), local))
+                    with torch.cuda.stream(self._stream):  # ordered after the backward, before the step
+                        dist.all_reduce(grads, group=group)
+                        grads.div_(world)
+                    _capi.check_mlp(self.L.lcb_mlp_adam_step(self._h, rate, 0.9, 0.999, 1e-8, 0.0))
                 step += 1
             v = C.c_double()
             _capi.check_mlp(self.L.lcb_mlp_take_loss(self._h, C.byref(v)))
@@ -250,6 +282,18 @@ class Surrogate:
                 log(f"epoch {ep} loss {losses[-1]:.3e} ({time.perf_counter() - t0:.1f} s)")
         self.train_seconds += time.perf_counter() - t0
         return losses
+
+    def _grads_tensor(self):
+        """The network's device gradient buffer as a torch tensor (no copy)."""
+        torch = _torch()
+        ptr, n = C.POINTER(C.c_float)(), C.c_int64()
+        _capi.check_mlp(self.L.lcb_mlp_grads_device(self._h, C.byref(ptr), C.byref(n)))
+
+        class _View:  # __cuda_array_interface__ of the library-owned buffer
+            __cuda_array_interface__ = {"shape": (n.value,), "typestr": "<f4", "version": 2,
+                                        "data": (C.cast(ptr, C.c_void_p).value, False), "strides": None}
+
+        return torch.as_tensor(_View(), device=self.dev)
 
     def _forward_dev(self, X):
         n = X.shape[0]

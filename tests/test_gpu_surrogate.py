@@ -136,3 +136,42 @@ def test_training_lowers_the_loss(lcb):
         assert losses[-1] < 0.1 * losses[0], losses
     finally:
         L.lcb_mlp_destroy(h)
+
+
+def test_data_parallel_path_matches_single_process(lcb):
+    """Surrogate.fit through its data-parallel path (backward, all-reduce of
+    lcb_mlp_grads_device on the network's stream, lcb_mlp_adam_step) in a
+    one-rank NCCL group: the kernels are deterministic and the reduction is
+    the identity, so the weights equal the default path's bit for bit."""
+    import importlib
+    import socket
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    S = importlib.import_module("lcurve-rs_b200.surrogate")
+    rng = np.random.default_rng(4)
+    theta = S.sample_prior(4096, seed=5)
+    phase = np.linspace(0.0, 1.0, 256)
+    flux = 1.0 + 0.2 * np.sin(2 * np.pi * phase[None, :] + 3 * theta[:, :1]) * theta[:, 2:3] / 0.03
+    flux *= 1.0 + 0.01 * rng.random(flux.shape)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        out = []
+        for group in (None, dist.group.WORLD):
+            sur = S.Surrogate(seed=3, max_batch=1024)
+            losses = sur.fit(theta, flux, epochs=3, batch=1024, group=group)
+            n = C.c_int64()
+            lcb._capi.check_mlp(sur.L.lcb_mlp_num_params(sur._h, C.byref(n)))
+            p = np.empty(n.value, np.float32)
+            lcb._capi.check_mlp(sur.L.lcb_mlp_get_params(sur._h, p.ctypes.data, n.value))
+            out.append((p, losses))
+        assert np.array_equal(out[0][0], out[1][0])
+        assert np.allclose(out[0][1], out[1][1], rtol=1e-9)  # the loss sum uses FP64 atomics
+        assert out[0][1][-1] < out[0][1][0]
+    finally:
+        dist.destroy_process_group()
