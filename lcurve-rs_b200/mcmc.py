@@ -30,6 +30,14 @@ delayed acceptance; with more sub-steps it is the surrogate transition method
 (Liu 2001, sec. 9.4.3).  Either way the pair of stages satisfies detailed
 balance with respect to the engine's posterior, so both samplers target the
 same distribution and the engine decides every accepted move.
+
+Multi-GPU: given a torch.distributed process group (one rank per GPU, every
+rank with the same seed, start and surrogate), both samplers shard the
+engine's work: every rank draws the same proposals, evaluates its contiguous
+share of the rows that need the engine, and an all-gather returns every
+row's log probability to every rank, so all ranks take the same decisions and
+hold the same chain as one process would.  `engine_evals` counts the rank's
+own evaluations.
 """
 from __future__ import annotations
 
@@ -159,24 +167,49 @@ class Run:
         return self.accepted / max(self.proposals, 1)
 
 
-def _eval_engine(engine, theta, chunk=128):
+def shard_bounds(n: int, world: int) -> list[int]:
+    """Row r of n belongs to rank k when bounds[k] <= r < bounds[k + 1]."""
+    return [k * n // world for k in range(world + 1)]
+
+
+def _gather_rows(local: np.ndarray, n: int, group) -> np.ndarray:
+    """All ranks' contiguous shards (shard_bounds) of n float64 values, in rank order."""
+    import torch  # noqa: PLC0415
+    import torch.distributed as dist  # noqa: PLC0415
+    world = dist.get_world_size(group)
+    b = shard_bounds(n, world)
+    width = max(b[k + 1] - b[k] for k in range(world))
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+    buf = torch.zeros(max(width, 1), dtype=torch.float64, device=dev)
+    buf[:local.shape[0]] = torch.as_tensor(local, dtype=torch.float64)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return np.concatenate([parts[k][:b[k + 1] - b[k]].cpu().numpy() for k in range(world)])
+
+
+def _eval_engine(engine, theta, chunk=128, group=None):
+    if group is not None:  # this rank's share, then every rank's values
+        import torch.distributed as dist  # noqa: PLC0415
+        b = shard_bounds(theta.shape[0], dist.get_world_size(group))
+        r = dist.get_rank(group)
+        return _gather_rows(_eval_engine(engine, theta[b[r]:b[r + 1]], chunk), theta.shape[0], group)
     out = np.full(theta.shape[0], -np.inf)
     for i in range(0, theta.shape[0], chunk):
         out[i:i + chunk] = _loglike(engine.chisq(theta[i:i + chunk], scale=True))
     return out
 
 
-def _eval_prob(engine, theta):
+def _eval_prob(engine, theta, group=None):
     lp = log_prior(theta)
     ok = np.isfinite(lp)
     out = np.full(theta.shape[0], -np.inf)
     if ok.any():
-        out[ok] = lp[ok] + _eval_engine(engine, theta[ok])
+        out[ok] = lp[ok] + _eval_engine(engine, theta[ok], group=group)
     return out
 
 
 def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0, move: str = "stretch",
-              bandwidth: float = 1.0) -> Run:
+              bandwidth: float = 1.0, group=None) -> Run:
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -184,7 +217,7 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
     chain = np.empty((nsteps, nw, d))
     t0 = time.perf_counter()
     ev0 = engine.evals
-    lp = _eval_prob(engine, x)
+    lp = _eval_prob(engine, x, group)
     acc = props = 0
     for s in range(nsteps):
         perm = rng.permutation(nw)
@@ -197,7 +230,7 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
             else:
                 y, z = _stretch(rng, x[S], x[Cc], a)
                 lratio = (d - 1) * np.log(z)
-            lpy = _eval_prob(engine, y)
+            lpy = _eval_prob(engine, y, group)
             loga = lratio + lpy - lp[S]
             take = np.log(rng.random(len(S))) < loga
             x[S[take]] = y[take]
@@ -210,7 +243,7 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
 
 def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0,
                 substeps: int = 1, device_subchain: bool | None = None, move: str = "stretch",
-                bandwidth: float = 1.0) -> Run:
+                bandwidth: float = 1.0, group=None) -> Run:
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -218,7 +251,7 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
     chain = np.empty((nsteps, nw, d))
     t0 = time.perf_counter()
     ev0 = engine.evals
-    lp = _eval_prob(engine, x)
+    lp = _eval_prob(engine, x, group)
     lps = log_prior(x) + _loglike(surrogate.chisq(x, scale=True))
     on_device = hasattr(surrogate, "subchain") if device_subchain is None else device_subchain
     acc = props = passed = nsur = 0
@@ -237,7 +270,7 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
             # stage 2: the engine decides for the walkers that moved
             if moved.any():
                 idx = np.nonzero(moved)[0]
-                lpy = log_prior(y[idx]) + _eval_engine(engine, y[idx])
+                lpy = log_prior(y[idx]) + _eval_engine(engine, y[idx], group=group)
                 loga2 = lpy - lp[S[idx]] - (lsy[idx] - lps[S[idx]])
                 take = np.log(rng.random(len(idx))) < loga2
                 w = S[idx[take]]

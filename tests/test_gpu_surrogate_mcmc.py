@@ -85,3 +85,36 @@ def test_trained_surrogate_gains_over_plain_mcmc(lcb, mods):
     per_eval = (_msjd(da, sig) / da.engine_evals) / (_msjd(plain, sig) / plain.engine_evals)
     per_s = (_msjd(da, sig) / da.seconds) / (_msjd(plain, sig) / plain.seconds)
     assert per_eval > 3.0 and per_s > 1.5, (per_eval, per_s, da.acceptance, plain.acceptance)
+
+
+def test_sharded_samplers_over_nccl_match_one_process(mods):
+    """The samplers' rank sharding through an NCCL group (device tensors in the
+    all-gather) of one rank: the chains of the unsharded run, exactly."""
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    S, M, _ = mods
+
+    class Quadratic:  # a cheap stand-in likelihood: only the sharding is under test here
+        evals = 0
+
+        def chisq(self, th, scale=True):
+            th = np.atleast_2d(th)
+            self.evals += th.shape[0]
+            return np.sum(((th - S.TRUTH) / (0.02 * (S.PRIOR_HI - S.PRIOR_LO))) ** 2, axis=1)
+
+    p0 = M.initial_walkers(32, S.TRUTH, seed=1, spread=0.02)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        a = M.run_plain(Quadratic(), p0, 30, seed=2, move="kde", group=dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+    b = M.run_plain(Quadratic(), p0, 30, seed=2, move="kde")
+    assert np.array_equal(a.chain, b.chain) and a.engine_evals == b.engine_evals

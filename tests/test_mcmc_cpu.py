@@ -97,3 +97,47 @@ def test_integrated_time_of_an_ar1_chain(M):
         x[t] = rho * x[t - 1] + rng.standard_normal((w, 1))
     tau = M.integrated_time(x)[0]
     assert abs(tau - (1 + rho) / (1 - rho)) < 0.1 * (1 + rho) / (1 - rho)
+
+
+def _sharded_worker(rank, world, port, out):
+    import os
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        out[rank] = _sharded_runs(dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+
+
+def _sharded_runs(group):
+    M = importlib.import_module("lcurve-rs_b200.mcmc")
+    S = importlib.import_module("lcurve-rs_b200.surrogate")
+    mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
+    eng = Gaussian(S, mu, 0.02)
+    p0 = M.initial_walkers(34, mu, seed=1, spread=0.02)  # halves of 17: uneven shards
+    plain = M.run_plain(eng, p0, 40, seed=2, move="kde", group=group)
+    da = M.run_delayed(eng, Gaussian(S, mu, 0.03, shift=0.7), p0, 40, seed=3, substeps=2, group=group)
+    return plain.chain, da.chain, plain.engine_evals, da.engine_evals
+
+
+def test_sharded_engine_evaluations_give_the_single_process_chains():
+    """Two gloo ranks, each evaluating its share of every batch of proposals:
+    both hold exactly the chains of one process, with the evaluations split."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = mp.Manager().dict()
+    mp.spawn(_sharded_worker, args=(2, port, out), nprocs=2, join=True)
+    single = _sharded_runs(None)
+    for r in (0, 1):
+        assert np.array_equal(out[r][0], single[0]) and np.array_equal(out[r][1], single[1])
+    assert out[0][2] + out[1][2] == single[2] and out[0][3] + out[1][3] == single[3]
+    assert 0 < out[0][2] < single[2]
