@@ -803,24 +803,33 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     for (int64_t i = 1; i < n && P.datum_contiguous; ++i)
         P.datum_contiguous = start[i] == start[i - 1] + std::max<int64_t>(count[i - 1], 0);
 
-    // global element / table layout (a model's segments are contiguous)
-    std::vector<size_t> seg_begin(n + 1);
+    // global element / table layout (a model's segments are contiguous): offsets of each model's
+    // segments, bands, rings and elements, then the tables filled in parallel
+    std::vector<size_t> seg_begin(n + 1, 0), band_begin(n + 1, 0), ring_begin(n + 1, 0);
+    std::vector<int64_t> elem_begin(n + 1, 0);
     for (int64_t i = 0; i < n; ++i) {
-        seg_begin[i] = P.segs.size();
-        ModelLayout& L = lay[i];
-        int32_t band0 = (int32_t)P.bands.size(), ring0 = (int32_t)P.rings.size();
-        P.bands.insert(P.bands.end(), L.bands.begin(), L.bands.end());
-        P.rings.insert(P.rings.end(), L.rings.begin(), L.rings.end());
-        for (SegDesc s : L.segs) {
-            s.first += P.nelem;
-            s.model = (int32_t)i;
-            if (s.kind == SEG_STAR1 || s.kind == SEG_STAR2) s.table += band0;
-            if (s.kind == SEG_DISC) s.table += ring0;
-            P.segs.push_back(s);
-        }
-        P.nelem += L.nelem;
+        seg_begin[i + 1] = seg_begin[i] + lay[i].segs.size();
+        band_begin[i + 1] = band_begin[i] + lay[i].bands.size();
+        ring_begin[i + 1] = ring_begin[i] + lay[i].rings.size();
+        elem_begin[i + 1] = elem_begin[i] + lay[i].nelem;
     }
-    seg_begin[n] = P.segs.size();
+    P.segs.resize(seg_begin[n]);
+    P.bands.resize(band_begin[n]);
+    P.rings.resize(ring_begin[n]);
+    P.nelem = elem_begin[n];
+    parallel_for(n, 8, [&](int64_t i) {
+        const ModelLayout& L = lay[i];
+        std::copy(L.bands.begin(), L.bands.end(), P.bands.begin() + band_begin[i]);
+        std::copy(L.rings.begin(), L.rings.end(), P.rings.begin() + ring_begin[i]);
+        size_t k = seg_begin[i];
+        for (SegDesc s : L.segs) {
+            s.first += elem_begin[i];
+            s.model = (int32_t)i;
+            if (s.kind == SEG_STAR1 || s.kind == SEG_STAR2) s.table += (int32_t)band_begin[i];
+            if (s.kind == SEG_DISC) s.table += (int32_t)ring_begin[i];
+            P.segs[k++] = s;
+        }
+    });
     if (P.nelem > ((int64_t)1 << 34)) throw Error(LCB_ERR_INVALID, "batch too large (elements)");
 
     // element-kernel blocks; Roche ray-march blocks (one per eclipsing Roche star); star-grid aux blocks:
@@ -937,23 +946,32 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         pbase += (int64_t)slot * D.nsub;
     }
     P.npartial = pbase;
-    // largest units first, ties in generation order: a stable two-pass radix sort
-    // (16 bits each) of the 32-bit keys INT32_MAX - size
-    thread_local std::vector<uint32_t> key, idx, tmp;
+    // largest units first, ties in generation order: a stable LSD radix sort of the keys
+    // largest - size (11-bit digits, keys carried with the indices; unit sizes are at most
+    // 16 chunks x one tile = 2^21 element-evals, so two passes)
+    thread_local std::vector<uint32_t> key, idx, ktmp, itmp;
     const size_t nu = fu.size();
+    int64_t largest = 0;
+    for (size_t k = 0; k < nu; ++k) largest = std::max(largest, std::min<int64_t>(fu[k].first, INT32_MAX));
     key.resize(nu);
     idx.resize(nu);
-    tmp.resize(nu);
+    ktmp.resize(nu);
+    itmp.resize(nu);
     for (size_t k = 0; k < nu; ++k) {
-        key[k] = (uint32_t)(INT32_MAX - std::min<int64_t>(fu[k].first, INT32_MAX));
+        key[k] = (uint32_t)(largest - std::min<int64_t>(fu[k].first, INT32_MAX));
         idx[k] = (uint32_t)k;
     }
-    for (int shift = 0; shift < 32; shift += 16) {
-        std::vector<size_t> count(65537, 0);
-        for (size_t k = 0; k < nu; ++k) ++count[((key[idx[k]] >> shift) & 0xffffu) + 1];
-        for (size_t b = 1; b < count.size(); ++b) count[b] += count[b - 1];
-        for (size_t k = 0; k < nu; ++k) tmp[count[(key[idx[k]] >> shift) & 0xffffu]++] = idx[k];
-        idx.swap(tmp);
+    for (int shift = 0; shift < 32 && (largest >> shift) > 0; shift += 11) {
+        uint32_t count[2049] = {0};
+        for (size_t k = 0; k < nu; ++k) ++count[((key[k] >> shift) & 2047u) + 1];
+        for (int b = 1; b <= 2048; ++b) count[b] += count[b - 1];
+        for (size_t k = 0; k < nu; ++k) {
+            const uint32_t pos = count[(key[k] >> shift) & 2047u]++;
+            ktmp[pos] = key[k];
+            itmp[pos] = idx[k];
+        }
+        key.swap(ktmp);
+        idx.swap(itmp);
     }
     P.units.resize(nu);
     for (size_t k = 0; k < nu; ++k) P.units[k] = fu[idx[k]].second;
