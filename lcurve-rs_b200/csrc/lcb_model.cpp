@@ -5,6 +5,7 @@
 #include "lcb_model.h"
 
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -315,13 +316,12 @@ std::string fmt_display(double v) {
     if (std::isnan(v)) return "NaN";
     if (std::isinf(v)) return v < 0 ? "-inf" : "inf";
     if (v == 0.0) return std::signbit(v) ? "-0" : "0";
-    // shortest digits that round-trip
+    // the shortest digits that round-trip, the closest to v among them (what Rust's Display
+    // prints; a "fewest printf digits that round-trip" search differs at powers of two, where
+    // the rounding interval is asymmetric)
     char buf[64];
-    int prec = 0;
-    for (; prec < 17; ++prec) {
-        std::snprintf(buf, sizeof buf, "%.*e", prec, v);
-        if (std::strtod(buf, nullptr) == v) break;
-    }
+    const auto r = std::to_chars(buf, buf + sizeof buf - 1, v, std::chars_format::scientific);
+    *r.ptr = '\0';
     std::string s(buf);
     bool neg = s[0] == '-';
     if (neg) s = s.substr(1);

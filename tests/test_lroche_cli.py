@@ -8,7 +8,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, ROOT, rust_disp, rust_e
 
 LROCHE = ROOT / "lcurve-rs_b200" / "lroche"
 
@@ -42,20 +42,9 @@ def test_golden_model_light_curve_file(tmp_path):
     assert np.max(np.abs(g[:, 2] - rf[:, 2]) / np.abs(rf[:, 2])) < 1e-5
     # each line formatted as main.rs:108-116 writes it: "{:20.15e} {} {:17.10e} {} {} {}"
     for line, row in zip(out.read_text().splitlines(), g):
-        want = " ".join([_rust_e(row[0], 15).rjust(20), _rust_disp(row[1]), _rust_e(row[2], 10).rjust(17),
-                         _rust_disp(row[3]), _rust_disp(row[4]), str(int(row[5]))])
+        want = " ".join([rust_e(row[0], 15).rjust(20), rust_disp(row[1]), rust_e(row[2], 10).rjust(17),
+                         rust_disp(row[3]), rust_disp(row[4]), str(int(row[5]))])
         assert line == want, (line, want)
-
-
-def _rust_e(x, prec):
-    """Rust's {:.Ne}: mantissa with N decimals, exponent without sign padding or zeros."""
-    mant, exp = f"{x:.{prec}e}".split("e")
-    return f"{mant}e{int(exp)}"
-
-
-def _rust_disp(x):
-    """Rust's Display of an f64: shortest round-trip digits, positional, no trailing .0."""
-    return np.format_float_positional(x, unique=True, trim="-")
 
 
 @pytest.mark.gpu
