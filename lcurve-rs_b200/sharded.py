@@ -1,0 +1,89 @@
+"""One model's light curve split across GPUs by time (one process per GPU).
+
+The data (times) of a single large model are divided into contiguous shards,
+one per rank of a torch.distributed process group (`mcmc.shard_bounds`).
+Each rank evaluates the whole model (grids, eclipses, continuum) and the flux
+sum for its own shard only, unscaled; the per-datum fluxes are all-gathered;
+then every rank applies the reference's single-factor scaling and
+chi-squared (orchestration.rs:264-310 with re_scale and compute_chisq,
+orchestration.rs:361-401) to the full set, in FP64.  The flux sum, which
+grows with elements x sub-phases, is divided among the ranks; the per-model
+work is repeated on each.  Each datum's flux depends on its own time alone,
+so the gathered fluxes are the unsplit evaluation's (to the flux sum's FP32
+rounding, which depends on how the batch is cut into work units).
+
+Models with per-component scale factors (iscale = 1) need the component
+fluxes of every datum for their SVD fit and are not split here.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import DATUM_DTYPE, LcResult, Result
+from .mcmc import _gather_rows, shard_bounds
+
+
+def re_scale(data: np.ndarray, fit: np.ndarray) -> tuple[float, float, float]:
+    """Single scale factor minimising chi-squared (orchestration.rs:361-389):
+    returns (scale, chisq, wnok) and scales `fit` in place."""
+    use = data["weight"] > 0.0
+    wgt = data["weight"][use] / data["ferr"][use] ** 2
+    sdy = float(np.sum(wgt * data["flux"][use] * fit[use]))
+    syy = float(np.sum(wgt * fit[use] * fit[use]))
+    wnok = float(np.sum(data["weight"][use]))
+    if wnok > 0.0 and syy > 0.0:
+        scale = sdy / syy
+        fit *= scale
+        chisq = float(np.sum(data["weight"][use] * ((data["flux"][use] - fit[use]) / data["ferr"][use]) ** 2))
+        return scale, chisq, wnok
+    return 1.0, 0.0, 0.0
+
+
+def compute_chisq(data: np.ndarray, calc: np.ndarray) -> tuple[float, float]:
+    """Weighted chi-squared and the weight sum (orchestration.rs:392-401)."""
+    use = data["weight"] > 0.0
+    chisq = float(np.sum(data["weight"][use] * ((data["flux"][use] - calc[use]) / data["ferr"][use]) ** 2))
+    return chisq, float(np.sum(data["weight"][use]))
+
+
+def _evaluate_engine(model, shard: np.ndarray):
+    r = model.light_curve(data=shard, scale=False)
+    return r.calc, dict(wdwarf=r.wdwarf, logg1=r.logg1, logg2=r.logg2, rv1=r.rv1, rv2=r.rv2)
+
+
+def light_curve_sharded(model, data: np.ndarray, scale: bool = False, group=None, evaluate=None) -> LcResult:
+    """Light curve of `model` at `data` (every rank passes the same) with the
+    flux sum divided among the ranks of `group` (None: this process alone);
+    returns what Model.light_curve(data=data, scale=scale) returns.
+
+    evaluate(model, shard) -> (unscaled fluxes, {wdwarf, logg1, logg2, rv1,
+    rv2}) computes one shard; by default the GPU engine through
+    Model.light_curve."""
+    data = np.ascontiguousarray(data, dtype=DATUM_DTYPE)
+    if evaluate is None:
+        if model.get_comp("iscale") not in ("0", "false"):
+            raise ValueError("per-component scaling (iscale = 1) is not split across ranks")
+        evaluate = _evaluate_engine
+    n = data.shape[0]
+    if group is None:
+        calc, per_model = evaluate(model, data)
+        calc = np.array(calc, dtype=np.float64)
+    else:
+        import torch.distributed as dist  # noqa: PLC0415
+        b = shard_bounds(n, dist.get_world_size(group))
+        r = dist.get_rank(group)
+        local, per_model = evaluate(model, data[b[r]:b[r + 1]]) if b[r + 1] > b[r] else (np.zeros(0), None)
+        if per_model is None:  # an empty shard still needs the model's own quantities
+            _, per_model = evaluate(model, data[:1])
+        calc = _gather_rows(np.asarray(local, dtype=np.float64), n, group)
+    res = Result()
+    res.logg1, res.logg2, res.rv1, res.rv2 = (per_model[k] for k in ("logg1", "logg2", "rv1", "rv2"))
+    if scale:  # orchestration.rs:282-287
+        s, res.chisq, res.wnok = re_scale(data, calc)
+    else:      # orchestration.rs:300-309 (sfac = 1)
+        s = 1.0
+        res.chisq, res.wnok = compute_chisq(data, calc)
+    res.wdwarf = per_model["wdwarf"] * s
+    for k in range(5):
+        res.sfac[k] = s
+    return LcResult(data["time"], calc, res)

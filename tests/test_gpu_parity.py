@@ -183,3 +183,37 @@ def test_iscale_components_and_svd_scale_vs_oracle(lcb, oracle, W, scale):
     assert res.wdwarf == pytest.approx(o_["wdwarf"], rel=tol)
     if scale:
         assert not np.allclose(o_["sfac"], 1.0)  # the fit moved the factors
+
+
+def test_time_split_light_curve_through_nccl_matches_light_curve(lcb):
+    """sharded.light_curve_sharded through a one-rank NCCL group (device
+    tensors in the all-gather) and without a group: the engine's own
+    light_curve(scale=True), up to the order of the FP64 scaling sums."""
+    import importlib
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    S = importlib.import_module("lcurve-rs_b200.sharded")
+    m = lcb.Model(GOLDEN / "test_model.dat")
+    t = np.linspace(-0.2, 1.2, 301)
+    d = lcb.make_data(t, expose=0.001, ndiv=1, ferr=0.01, weight=1.0)
+    d["flux"] = 0.02 + 0.005 * np.cos(2 * np.pi * t)
+    d["weight"][::17] = 0.0
+    ref = m.light_curve(data=d, scale=True)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        a = S.light_curve_sharded(m, d, scale=True, group=dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+    b = S.light_curve_sharded(m, d, scale=True)
+    for r in (a, b):
+        assert np.allclose(r.calc, ref.calc, rtol=1e-12, atol=0)
+        assert np.isclose(r.chisq, ref.chisq, rtol=1e-12) and r.wnok == ref.wnok
+        assert np.isclose(r.wdwarf, ref.wdwarf, rtol=1e-12) and np.allclose(r.sfac, ref.sfac, rtol=1e-12)
