@@ -2379,6 +2379,19 @@ double orc_xl12(double q, double s) { try { return xl12(q, s); } catch (...) { r
 double orc_planck(double w, double t) { return planck(w, t); }
 double orc_dlpdlt(double w, double t) { return dlpdlt(w, t); }
 int64_t orc_numface(int nlat) { return numface(nlat, false, 0.0, 0.0, 0, 0); }
+// svd_scale (orchestration.rs:405-436) on caller-supplied component fluxes (fcomp: n x ncol,
+// row-major), for checks of the least-squares restatement itself.
+void orc_svd_scale(const double* flux, const double* ferr, const double* weight, int n, const double* fcomp,
+                   int ncol, double* out) {
+    std::vector<Datum> data(n);
+    std::vector<std::vector<double>> fc(n, std::vector<double>(ncol));
+    for (int i = 0; i < n; ++i) {
+        data[i].flux = flux[i]; data[i].ferr = ferr[i]; data[i].weight = weight[i];
+        for (int j = 0; j < ncol; ++j) fc[i][j] = fcomp[(size_t)i * ncol + j];
+    }
+    std::vector<double> x = svd_scale(data, fc, ncol);
+    for (int j = 0; j < ncol; ++j) out[j] = x[j];
+}
 void orc_stream_spot(double q, double rad, double* out3) {
     Vec3 r, v;
     strinit(q, r, v);

@@ -66,6 +66,7 @@ def lib():
     L.orc_numface.argtypes = [ip]
     L.orc_numface.restype = C.c_int64
     L.orc_stream_spot.argtypes = [C.c_double, C.c_double, dp]
+    L.orc_svd_scale.argtypes = [dp, dp, dp, ip, dp, ip, dp]
     L.orc_star_eclipse.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
                                    C.c_double, ip, ip, dp, dp]
     L.orc_counters.argtypes = [C.POINTER(C.c_longlong)]

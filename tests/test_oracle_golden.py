@@ -105,3 +105,54 @@ def test_chisq_batch_unphysical_is_nan(oracle, test_model_path):
     d = oracle.make_data(t, flux=0.0, ferr=1.0, weight=1.0)
     out = m.chisq_batch(d, ["r2"], np.array([[0.99]]))
     assert np.isnan(out[0])
+
+
+def _svd_lstsq(flux, ferr, weight, fcomp):
+    """svd_scale restated through LAPACK's SVD: rows with weight > 0 scaled by
+    sqrt(weight) / ferr, x = V S^+ U^T b with singular values below 1e-12
+    (absolute, as nalgebra's SVD::solve(b, 1e-12)) treated as zero."""
+    use = weight > 0
+    ncol = fcomp.shape[1]
+    if use.sum() < ncol or use.sum() == 0:
+        return np.ones(ncol)
+    w = np.sqrt(weight[use]) / ferr[use]
+    a, b = fcomp[use] * w[:, None], flux[use] * w
+    u, s, vt = np.linalg.svd(a, full_matrices=False)
+    keep = s >= 1e-12
+    return vt.T[:, keep] @ ((u.T[keep] @ b) / s[keep])
+
+
+def test_svd_scale_restatement_against_lapack(oracle):
+    """The oracle's one-sided Jacobi least squares (svd_scale, the iscale = 1
+    path; orchestration.rs:405-436) against the same problem solved through
+    LAPACK: well-conditioned, an all-zero component (singular value 0: its
+    factor is 0), two identical components (the minimum-norm split) and too
+    few weighted rows (all ones)."""
+    import ctypes as C
+    L = oracle.lib()
+    rng = np.random.default_rng(9)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    cases = []
+    for ncol in (4, 5):
+        n = 300
+        fcomp = np.abs(rng.normal(1.0, 0.5, (n, ncol))) * np.array([1.0, 0.3, 0.05, 0.02, 0.5])[:ncol]
+        truth = rng.uniform(0.5, 2.0, ncol)
+        ferr = rng.uniform(0.005, 0.02, n)
+        flux = fcomp @ truth + rng.normal(0.0, 1.0, n) * ferr
+        weight = np.where(rng.random(n) < 0.1, 0.0, rng.uniform(0.5, 2.0, n))
+        cases.append((flux, ferr, weight, fcomp, 1e-10))
+        zero = fcomp.copy()
+        zero[:, 2] = 0.0
+        cases.append((zero @ truth, ferr, weight, zero, 1e-10))
+        twin = fcomp.copy()
+        twin[:, 1] = twin[:, 0]
+        cases.append((twin @ truth, ferr, weight, twin, 1e-8))
+    few = np.ones((3, 5))
+    cases.append((np.ones(3), np.ones(3), np.ones(3), few, 0.0))
+    for flux, ferr, weight, fcomp, tol in cases:
+        out = np.zeros(fcomp.shape[1])
+        fc = np.ascontiguousarray(fcomp)
+        L.orc_svd_scale(dp(np.ascontiguousarray(flux)), dp(np.ascontiguousarray(ferr)),
+                        dp(np.ascontiguousarray(weight)), fcomp.shape[0], dp(fc), fcomp.shape[1], dp(out))
+        ref = _svd_lstsq(flux, ferr, weight, fcomp)
+        assert np.allclose(out, ref, rtol=tol, atol=tol * np.max(np.abs(ref))), (out, ref)
