@@ -2379,6 +2379,47 @@ double orc_xl12(double q, double s) { try { return xl12(q, s); } catch (...) { r
 double orc_planck(double w, double t) { return planck(w, t); }
 double orc_dlpdlt(double w, double t) { return dlpdlt(w, t); }
 int64_t orc_numface(int nlat) { return numface(nlat, false, 0.0, 0.0, 0, 0); }
+// Roche-geometry helpers of the reference's roche crate, for its unit-test known answers.
+double orc_rpot(double q, double x, double y, double z) { return rpot(q, Vec3(x, y, z)); }
+void orc_drpot1(double q, double spin, double x, double y, double z, double* out3) {
+    Vec3 g = drpot1(q, spin, Vec3(x, y, z));
+    out3[0] = g.x; out3[1] = g.y; out3[2] = g.z;
+}
+void orc_set_earth(double iangle, double phase, double* out3) {  // misc.rs:36-39
+    const double irad = iangle * (PI / 180.0);  // f64::to_radians
+    Vec3 e = set_earth_cosi_sini(std::cos(irad), std::sin(irad), phase);
+    out3[0] = e.x; out3[1] = e.y; out3[2] = e.z;
+}
+void orc_strinit(double q, double* r3, double* v3) {
+    Vec3 r, v;
+    strinit(q, r, v);
+    r3[0] = r.x; r3[1] = r.y; r3[2] = r.z; v3[0] = v.x; v3[1] = v.y; v3[2] = v.z;
+}
+// One gsint step of size ttry from strinit, for the Jacobi-constant check (stream.rs:292-309):
+// the stream state before (rv0) and after (rv1) the step, 6 values each.
+void orc_gsint_step(double q, double ttry, double eps, double* rv0, double* rv1) {
+    Vec3 r, v;
+    strinit(q, r, v);
+    rv0[0] = r.x; rv0[1] = r.y; rv0[2] = r.z; rv0[3] = v.x; rv0[4] = v.y; rv0[5] = v.z;
+    BsState st;
+    double time = 0.0, tdid = 0.0, tnext = 0.0;
+    gsint(q, r, v, ttry, time, eps, st, tdid, tnext);
+    rv1[0] = r.x; rv1[1] = r.y; rv1[2] = r.z; rv1[3] = v.x; rv1[4] = v.y; rv1[5] = v.z;
+}
+void orc_ref_sphere(double q, int secondary, double spin, double ffac, double* rref_pref) {
+    ref_sphere(q, secondary ? SECONDARY : PRIMARY, spin, ffac, rref_pref[0], rref_pref[1]);
+}
+// face (surface.rs:54-121) of the star in direction dirn: point, normal, radius and gravity.
+void orc_face(double q, int secondary, double spin, double ffac, const double* dirn, double acc, double* pvec3,
+              double* dvec3, double* r_g) {
+    double rref = 0.0, pref = 0.0;
+    const Star star = secondary ? SECONDARY : PRIMARY;
+    ref_sphere(q, star, spin, ffac, rref, pref);
+    Vec3 pvec, dvec;
+    face(q, star, spin, Vec3(dirn[0], dirn[1], dirn[2]), rref, pref, acc, pvec, dvec, r_g[0], r_g[1]);
+    pvec3[0] = pvec.x; pvec3[1] = pvec.y; pvec3[2] = pvec.z;
+    dvec3[0] = dvec.x; dvec3[1] = dvec.y; dvec3[2] = dvec.z;
+}
 // svd_scale (orchestration.rs:405-436) on caller-supplied component fluxes (fcomp: n x ncol,
 // row-major), for checks of the least-squares restatement itself.
 void orc_svd_scale(const double* flux, const double* ferr, const double* weight, int n, const double* fcomp,

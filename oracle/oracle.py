@@ -67,6 +67,14 @@ def lib():
     L.orc_numface.restype = C.c_int64
     L.orc_stream_spot.argtypes = [C.c_double, C.c_double, dp]
     L.orc_svd_scale.argtypes = [dp, dp, dp, ip, dp, ip, dp]
+    L.orc_rpot.argtypes = [C.c_double] * 4
+    L.orc_rpot.restype = C.c_double
+    L.orc_drpot1.argtypes = [C.c_double] * 5 + [dp]
+    L.orc_set_earth.argtypes = [C.c_double, C.c_double, dp]
+    L.orc_strinit.argtypes = [C.c_double, dp, dp]
+    L.orc_gsint_step.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
+    L.orc_ref_sphere.argtypes = [C.c_double, ip, C.c_double, C.c_double, dp]
+    L.orc_face.argtypes = [C.c_double, ip, C.c_double, C.c_double, dp, C.c_double, dp, dp, dp]
     L.orc_star_eclipse.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
                                    C.c_double, ip, ip, dp, dp]
     L.orc_counters.argtypes = [C.POINTER(C.c_longlong)]

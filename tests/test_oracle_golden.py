@@ -156,3 +156,47 @@ def test_svd_scale_restatement_against_lapack(oracle):
                         dp(np.ascontiguousarray(weight)), fcomp.shape[0], dp(fc), fcomp.shape[1], dp(out))
         ref = _svd_lstsq(flux, ferr, weight, fcomp)
         assert np.allclose(out, ref, rtol=tol, atol=tol * np.max(np.abs(ref))), (out, ref)
+
+
+def test_roche_unit_known_answers(oracle):
+    """The reference roche crate's own unit tests, on the oracle's restatements:
+    set_earth at i = 90 (misc.rs:58-69), the potential's sign (potential.rs:
+    133-142), zero gradient at L1 (potential.rs:145-152), strinit just inside
+    L1 (stream.rs:282-289) and the Jacobi constant over one gsint step
+    (stream.rs:292-309; jacobi from misc.rs:21-28), ref_sphere and face on the
+    primary (surface.rs:128-146)."""
+    import ctypes as C
+    L = oracle.lib()
+    v3 = lambda: (C.c_double * 3)()  # noqa: E731
+    e = v3()
+    L.orc_set_earth(90.0, 0.0, e)
+    assert abs(e[0] - 1.0) < 1e-10 and abs(e[1]) < 1e-10 and abs(e[2]) < 1e-10
+    L.orc_set_earth(90.0, 0.25, e)
+    assert abs(e[0]) < 1e-10 and abs(e[1] + 1.0) < 1e-10
+    assert math.isfinite(L.orc_rpot(1.0, 0.5, 0.0, 0.0))
+    assert L.orc_rpot(1.0, 0.1, 0.0, 0.0) < 0.0
+    g = v3()
+    L.orc_drpot1(1.0, 1.0, L.orc_xl1(1.0), 0.0, 0.0, g)
+    assert abs(g[0]) < 1e-10 and abs(g[1]) < 1e-15 and abs(g[2]) < 1e-15
+    r, v = v3(), v3()
+    L.orc_strinit(1.0, r, v)
+    assert 0.0 < r[0] < 0.5 and abs(r[1]) < 0.01 and r[2] == 0.0 and v[0] < 0.0
+
+    def jacobi(q, s):
+        f1 = 1.0 / (1.0 + q)
+        f2 = f1 * q
+        yzsq = s[1] ** 2 + s[2] ** 2
+        return ((s[3] ** 2 + s[4] ** 2 + s[5] ** 2 - s[1] ** 2 - (s[0] - f2) ** 2) / 2.0
+                - f1 / math.sqrt(s[0] ** 2 + yzsq) - f2 / math.sqrt((s[0] - 1.0) ** 2 + yzsq))
+
+    s0, s1 = (C.c_double * 6)(), (C.c_double * 6)()
+    L.orc_gsint_step(0.5, 0.01, 1e-10, s0, s1)
+    assert list(s0) != list(s1)
+    assert abs(jacobi(0.5, s0) - jacobi(0.5, s1)) < 1e-8
+    # ref_sphere and face (surface.rs:128-146)
+    rp = (C.c_double * 2)()
+    L.orc_ref_sphere(1.0, 1, 1.0, 1.0, rp)
+    assert rp[0] > 0.0 and rp[1] < 0.0
+    p, d, rg = v3(), v3(), (C.c_double * 2)()
+    L.orc_face(0.5, 0, 1.0, 0.9, (C.c_double * 3)(0.0, 1.0, 0.0), 1e-6, p, d, rg)
+    assert rg[0] > 0.0 and rg[1] > 0.0 and p[1] > 0.0
