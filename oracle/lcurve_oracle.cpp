@@ -2420,6 +2420,22 @@ void orc_face(double q, int secondary, double spin, double ffac, const double* d
     pvec3[0] = pvec.x; pvec3[1] = pvec.y; pvec3[2] = pvec.z;
     dvec3[0] = dvec.x; dvec3[1] = dvec.y; dvec3[2] = dvec.z;
 }
+// dbrent (dbrent.rs:20-169) on f(x) = (x - 3)^2 + 1 from the bracket (0, 2, 6) (dbrent.rs:172-181).
+int orc_dbrent_quadratic(double* fmin_xmin) {
+    auto f = [](double x) { return (x - 3.0) * (x - 3.0) + 1.0; };
+    auto df = [](double x) { return 2.0 * (x - 3.0); };
+    return dbrent(0.0, 2.0, 6.0, f, df, 1e-10, false, 0.0, fmin_xmin[0], fmin_xmin[1]) ? 1 : 0;
+}
+// One bsstep (bsstep.rs:159-326) of dy/dx = y from y(0) = 1 with htry = 1 (bsstep.rs:570-597):
+// returns y and the x reached.
+void orc_bsstep_exp(double* y_x) {
+    double y[1] = {1.0}, dydx[1] = {1.0}, yscal[1] = {1.0}, xx = 0.0, hdid = 0.0, hnext = 0.0;
+    BsState st;
+    Derivs d = [](double, const double* yi, double* dy) { dy[0] = yi[0]; };
+    bsstep(y, dydx, 1, xx, 1.0, 1e-10, yscal, st, d, hdid, hnext);
+    y_x[0] = y[0];
+    y_x[1] = xx;
+}
 // svd_scale (orchestration.rs:405-436) on caller-supplied component fluxes (fcomp: n x ncol,
 // row-major), for checks of the least-squares restatement itself.
 void orc_svd_scale(const double* flux, const double* ferr, const double* weight, int n, const double* fcomp,

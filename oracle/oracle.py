@@ -75,6 +75,8 @@ def lib():
     L.orc_gsint_step.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
     L.orc_ref_sphere.argtypes = [C.c_double, ip, C.c_double, C.c_double, dp]
     L.orc_face.argtypes = [C.c_double, ip, C.c_double, C.c_double, dp, C.c_double, dp, dp, dp]
+    L.orc_dbrent_quadratic.argtypes = [dp]
+    L.orc_bsstep_exp.argtypes = [dp]
     L.orc_star_eclipse.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
                                    C.c_double, ip, ip, dp, dp]
     L.orc_counters.argtypes = [C.POINTER(C.c_longlong)]

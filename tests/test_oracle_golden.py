@@ -200,3 +200,18 @@ def test_roche_unit_known_answers(oracle):
     p, d, rg = v3(), v3(), (C.c_double * 2)()
     L.orc_face(0.5, 0, 1.0, 0.9, (C.c_double * 3)(0.0, 1.0, 0.0), 1e-6, p, d, rg)
     assert rg[0] > 0.0 and rg[1] > 0.0 and p[1] > 0.0
+
+
+def test_numerical_known_answers(oracle):
+    """The subs crate's numerical unit tests on the oracle's restatements:
+    dbrent finds the minimum of (x - 3)^2 + 1 from (0, 2, 6) (dbrent.rs:
+    172-181); one Bulirsch-Stoer step of dy/dx = y matches e^x at the x it
+    reached (bsstep.rs:570-597)."""
+    import ctypes as C
+    L = oracle.lib()
+    fx = (C.c_double * 2)()
+    assert L.orc_dbrent_quadratic(fx) in (0, 1)
+    assert abs(fx[1] - 3.0) < 1e-9 and abs(fx[0] - 1.0) < 1e-9
+    yx = (C.c_double * 2)()
+    L.orc_bsstep_exp(yx)
+    assert yx[1] > 0.0 and abs(yx[0] - math.exp(yx[1])) / math.exp(yx[1]) < 1e-8
