@@ -12,6 +12,9 @@ physically invalid model (r2 = 0.99, orchestration.rs:350-354 -> NaN).
 * element / Roche / aux blocks cover their segments;
 * an invalid model is marked failed and owns no elements;
 * re-planning into the same (reused) storage reproduces the plan exactly.
+
+And the planner's FP64 helpers (L1 points, the bright-spot stream, grid
+element counts) against the oracle's separate restatements.
 """
 import shutil
 import subprocess
@@ -183,3 +186,48 @@ def test_plan_invariants(driver):
     r = subprocess.run([str(driver / "d"), str(driver / "models.bin")], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "failed 1 " in r.stdout, r.stdout
+
+
+HELPERS = r"""
+#include <cstdio>
+#include <cstdlib>
+#include "lcb_plan.h"
+int main(int argc, char** argv) {
+    // argv: q spin rad nlat, one case per 4 arguments
+    for (int i = 1; i + 3 < argc; i += 4) {
+        const double q = std::atof(argv[i]), spin = std::atof(argv[i + 1]), rad = std::atof(argv[i + 2]);
+        const int nlat = std::atoi(argv[i + 3]);
+        double s[3];
+        lcb::host_stream_spot(q, rad, s);
+        std::printf("%.17g %.17g %.17g %.17g %.17g %.17g %lld\n", lcb::host_xl1(q), lcb::host_xl11(q, spin),
+                    lcb::host_xl12(q, spin), s[0], s[1], s[2], (long long)lcb::host_numface(nlat));
+    }
+}
+"""
+
+
+def test_host_geometry_helpers_match_the_oracle(driver, oracle):
+    """The planner's own FP64 helpers (L1 points, the bright-spot stream
+    integration, star-grid element counts) against the oracle's separate
+    restatements (lagrange.rs, stream.rs:82-145, grid.rs:8-46)."""
+    import ctypes as C
+    (driver / "h.cpp").write_text(HELPERS)
+    src = ROOT / "lcurve-rs_b200" / "csrc"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I/usr/local/cuda/include", f"-I{src}", str(driver / "h.cpp"),
+                    str(src / "lcb_plan.cpp"), str(src / "lcb_model.cpp"), "-o", str(driver / "h"), "-lpthread"],
+                   check=True)
+    L = oracle.lib()
+    # spot radii the stream crosses on its way in from L1 (fractions of the L1 distance)
+    cases = [(q, spin, round(frac * L.orc_xl1(q), 6), nlat) for q in (0.08, 0.3, 0.7, 1.0)
+             for spin, frac, nlat in ((1.0, 0.35, 20), (0.8, 0.55, 57), (1.2, 0.8, 300))]
+    args = [str(v) for c in cases for v in c]
+    out = subprocess.run([str(driver / "h")] + args, capture_output=True, text=True, check=True).stdout.splitlines()
+    for (q, spin, rad, nlat), line in zip(cases, out):
+        f = line.split()
+        xl1, xl11, xl12, sx, sy, sz = (float(x) for x in f[:6])
+        assert abs(xl1 - L.orc_xl1(q)) < 1e-12
+        assert abs(xl11 - L.orc_xl11(q, spin)) < 1e-12 and abs(xl12 - L.orc_xl12(q, spin)) < 1e-12
+        ref = (C.c_double * 3)()
+        L.orc_stream_spot(q, rad, ref)
+        assert max(abs(sx - ref[0]), abs(sy - ref[1]), abs(sz - ref[2])) < 1e-10, (q, rad)
+        assert int(f[6]) == L.orc_numface(nlat)
