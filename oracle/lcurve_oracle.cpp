@@ -2380,10 +2380,16 @@ double orc_planck(double w, double t) { return planck(w, t); }
 double orc_dlpdlt(double w, double t) { return dlpdlt(w, t); }
 int64_t orc_numface(int nlat) { return numface(nlat, false, 0.0, 0.0, 0, 0); }
 // Roche-geometry helpers of the reference's roche crate, for its unit-test known answers.
-double orc_rpot(double q, double x, double y, double z) { return rpot(q, Vec3(x, y, z)); }
+double orc_rpot(double q, double x, double y, double z) {
+    try { return rpot(q, Vec3(x, y, z)); } catch (const std::exception&) { return NAN; }
+}
 void orc_drpot1(double q, double spin, double x, double y, double z, double* out3) {
-    Vec3 g = drpot1(q, spin, Vec3(x, y, z));
-    out3[0] = g.x; out3[1] = g.y; out3[2] = g.z;
+    try {
+        Vec3 g = drpot1(q, spin, Vec3(x, y, z));
+        out3[0] = g.x; out3[1] = g.y; out3[2] = g.z;
+    } catch (const std::exception&) {
+        out3[0] = out3[1] = out3[2] = NAN;
+    }
 }
 void orc_set_earth(double iangle, double phase, double* out3) {  // misc.rs:36-39
     const double irad = iangle * (PI / 180.0);  // f64::to_radians
@@ -2391,34 +2397,51 @@ void orc_set_earth(double iangle, double phase, double* out3) {  // misc.rs:36-3
     out3[0] = e.x; out3[1] = e.y; out3[2] = e.z;
 }
 void orc_strinit(double q, double* r3, double* v3) {
-    Vec3 r, v;
-    strinit(q, r, v);
-    r3[0] = r.x; r3[1] = r.y; r3[2] = r.z; v3[0] = v.x; v3[1] = v.y; v3[2] = v.z;
+    try {
+        Vec3 r, v;
+        strinit(q, r, v);
+        r3[0] = r.x; r3[1] = r.y; r3[2] = r.z; v3[0] = v.x; v3[1] = v.y; v3[2] = v.z;
+    } catch (const std::exception&) {
+        for (int k = 0; k < 3; ++k) r3[k] = v3[k] = NAN;
+    }
 }
 // One gsint step of size ttry from strinit, for the Jacobi-constant check (stream.rs:292-309):
 // the stream state before (rv0) and after (rv1) the step, 6 values each.
 void orc_gsint_step(double q, double ttry, double eps, double* rv0, double* rv1) {
-    Vec3 r, v;
-    strinit(q, r, v);
-    rv0[0] = r.x; rv0[1] = r.y; rv0[2] = r.z; rv0[3] = v.x; rv0[4] = v.y; rv0[5] = v.z;
-    BsState st;
-    double time = 0.0, tdid = 0.0, tnext = 0.0;
-    gsint(q, r, v, ttry, time, eps, st, tdid, tnext);
-    rv1[0] = r.x; rv1[1] = r.y; rv1[2] = r.z; rv1[3] = v.x; rv1[4] = v.y; rv1[5] = v.z;
+    try {
+        Vec3 r, v;
+        strinit(q, r, v);
+        rv0[0] = r.x; rv0[1] = r.y; rv0[2] = r.z; rv0[3] = v.x; rv0[4] = v.y; rv0[5] = v.z;
+        BsState st;
+        double time = 0.0, tdid = 0.0, tnext = 0.0;
+        gsint(q, r, v, ttry, time, eps, st, tdid, tnext);
+        rv1[0] = r.x; rv1[1] = r.y; rv1[2] = r.z; rv1[3] = v.x; rv1[4] = v.y; rv1[5] = v.z;
+    } catch (const std::exception&) {
+        for (int k = 0; k < 6; ++k) rv0[k] = rv1[k] = NAN;
+    }
 }
 void orc_ref_sphere(double q, int secondary, double spin, double ffac, double* rref_pref) {
-    ref_sphere(q, secondary ? SECONDARY : PRIMARY, spin, ffac, rref_pref[0], rref_pref[1]);
+    try {
+        ref_sphere(q, secondary ? SECONDARY : PRIMARY, spin, ffac, rref_pref[0], rref_pref[1]);
+    } catch (const std::exception&) {
+        rref_pref[0] = rref_pref[1] = NAN;
+    }
 }
 // face (surface.rs:54-121) of the star in direction dirn: point, normal, radius and gravity.
 void orc_face(double q, int secondary, double spin, double ffac, const double* dirn, double acc, double* pvec3,
               double* dvec3, double* r_g) {
-    double rref = 0.0, pref = 0.0;
-    const Star star = secondary ? SECONDARY : PRIMARY;
-    ref_sphere(q, star, spin, ffac, rref, pref);
-    Vec3 pvec, dvec;
-    face(q, star, spin, Vec3(dirn[0], dirn[1], dirn[2]), rref, pref, acc, pvec, dvec, r_g[0], r_g[1]);
-    pvec3[0] = pvec.x; pvec3[1] = pvec.y; pvec3[2] = pvec.z;
-    dvec3[0] = dvec.x; dvec3[1] = dvec.y; dvec3[2] = dvec.z;
+    try {
+        double rref = 0.0, pref = 0.0;
+        const Star star = secondary ? SECONDARY : PRIMARY;
+        ref_sphere(q, star, spin, ffac, rref, pref);
+        Vec3 pvec, dvec;
+        face(q, star, spin, Vec3(dirn[0], dirn[1], dirn[2]), rref, pref, acc, pvec, dvec, r_g[0], r_g[1]);
+        pvec3[0] = pvec.x; pvec3[1] = pvec.y; pvec3[2] = pvec.z;
+        dvec3[0] = dvec.x; dvec3[1] = dvec.y; dvec3[2] = dvec.z;
+    } catch (const std::exception&) {
+        for (int k = 0; k < 3; ++k) pvec3[k] = dvec3[k] = NAN;
+        r_g[0] = r_g[1] = NAN;
+    }
 }
 // dbrent (dbrent.rs:20-169) on f(x) = (x - 3)^2 + 1 from the bracket (0, 2, 6) (dbrent.rs:172-181).
 int orc_dbrent_quadratic(double* fmin_xmin) {
@@ -2449,11 +2472,17 @@ void orc_svd_scale(const double* flux, const double* ferr, const double* weight,
     std::vector<double> x = svd_scale(data, fc, ncol);
     for (int j = 0; j < ncol; ++j) out[j] = x[j];
 }
+// The exports below return NaNs where the reference raises an error (an unreachable
+// radius, an invalid q): an exception must not cross the C boundary.
 void orc_stream_spot(double q, double rad, double* out3) {
-    Vec3 r, v;
-    strinit(q, r, v);
-    stradv(q, r, v, rad, 1e-10, 1e-3);
-    out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
+    try {
+        Vec3 r, v;
+        strinit(q, r, v);
+        stradv(q, r, v, rad, 1e-10, 1e-3);
+        out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
+    } catch (const std::exception&) {
+        out3[0] = out3[1] = out3[2] = NAN;
+    }
 }
 // Per-element star-eclipse interval (for parity of the eclipse kernel on arbitrary points).
 int orc_star_eclipse(double q, double r, double spin, double ffac, double iangle, const double* posn, double delta,

@@ -68,6 +68,9 @@ def test_stream_spot_position(oracle):
     r = math.sqrt(out[0] ** 2 + out[1] ** 2 + out[2] ** 2)
     assert abs(r - 0.3) < 1e-9
     assert out[2] == 0.0
+    # a radius the stream never reaches is the reference's error (stream.rs:139-141): NaN here
+    oracle.lib().orc_stream_spot(0.08, 0.12, out)
+    assert all(math.isnan(x) for x in out)
 
 
 def test_parse_errors(oracle, tmp_path):
