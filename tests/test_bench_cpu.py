@@ -57,3 +57,26 @@ def test_reference_arm_runs_on_rank_0_only(capsys):
         pass
     assert bench.run_reference(Args(), rank=1, world=2) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the oracle on the host cores) prints one JSON
+    line with the metric, unit and config of the GPU arm, its own cpu_baseline
+    and an e2e with no device transfers."""
+    import json
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "0",
+                        "--cpu-sample", "1"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    import bench
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["steps"] == 1
+    assert line["config"]["workload"].startswith("batch_1024")
+    cpu = line["cpu_baseline"]
+    assert cpu["value"] == line["value"] and cpu["kind"] == "port" and cpu["cores"] >= 1 and cpu["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
