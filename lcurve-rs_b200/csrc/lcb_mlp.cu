@@ -9,26 +9,32 @@
 //
 // GEMM kernel (k_gemm): C[M x N] = A[M x K] . B[N x K]^T, both operands BF16
 // row-major (K contiguous), FP32 accumulation in tensor memory:
-//   - one CTA per 128 x 128 output tile, four warps;
-//   - warp 0 lane 0 streams 128 x 64 K-slices of A and B into shared memory
+//   - one CTA per 128 x TBN output tile (TBN = 256 when N >= 256, else 128),
+//     sixteen warps; a K-split grid (blockIdx.z) for FP32 outputs;
+//   - warp 0 lane 0 streams 64-wide K-slices of A and B into shared memory
 //     with TMA (cp.async.bulk.tensor, 128-byte swizzle), four stages on
 //     mbarriers;
-//   - warp 1 lane 0 issues tcgen05.mma (kind::f16, M=128, N=128, K=16) from
-//     shared-memory descriptors into a 128-column TMEM accumulator, and
+//   - warp 1 lane 0 issues tcgen05.mma (kind::f16, M=128, N=TBN, K=16) from
+//     shared-memory descriptors into a TBN-column TMEM accumulator, and
 //     releases each stage with tcgen05.commit;
-//   - all four warps read the accumulator back with tcgen05.ld (warp w owns
-//     TMEM lanes 32w..32w+31 = tile rows) and apply the fused epilogue:
+//   - every warp reads the accumulator back with tcgen05.ld (warp w: TMEM
+//     lanes 32 (w % 4) .. + 31 = tile rows, every fourth 32-column chunk from
+//     w / 4), applies the fused epilogue and stages each 32 x 32 chunk in the
+//     idle operand buffers so the global stores are row-contiguous:
 //       EPI_F32        out = acc                                  (weight gradients)
 //       EPI_BIAS_GELU  z = acc + bias; out = bf16(gelu(z)); out2 = z  (hidden layers)
 //       EPI_BIAS_F32   out = acc + bias                           (output layer)
 //       EPI_DGELU      out = bf16(acc * gelu'(aux))               (backward through GELU)
+//     the two BF16 modes optionally also write out transposed (outT).
 // Every mbarrier wait is bounded; a time-out sets the error word and the CTA
 // still releases its tensor memory.
 //
-// Training runs forward, backward (weight gradients as dZ^T . X with both
-// operands transposed into K-major copies, input gradients as dZ . W^T with a
-// transposed weight copy kept by the optimiser) and Adam on FP32 master
-// weights; every step is a fixed launch sequence on the network's stream.
+// Training runs forward (keeping each hidden activation transposed as well),
+// backward (weight gradients dZ^T . X over K = batch split across the SMs and
+// summed in a fixed order; bias gradients as row sums of dZ^T; input gradients
+// dZ . W^T through the dGELU epilogue, which also writes dZ^T for the next
+// layer) and Adam on FP32 master weights; every step is a fixed launch
+// sequence on the network's stream.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
