@@ -1,27 +1,38 @@
-// lcb_kernels.cu — sm_100a kernels of the light-curve path.
+// lcb_kernels.cu — sm_100a kernels of the light-curve path, in launch order.
 //
-//   k_elements : one thread per grid element of every model in the batch.
-//                Surface point (surface.rs:54-121) or sphere point, area,
-//                gravity (grid.rs:201-322; disc/rim/spot grid.rs:336-553);
-//                eclipse intervals by the other star -- FP64 Roche ray-march
-//                ingress_egress (eclipse.rs:270-373) or the analytic sphere
-//                case (eclipse.rs:229-265) -- and by an opaque disc
-//                (disc_eclipse.rs:84-330); continuum flux (brightness.rs);
-//                per-model FP64 reductions for ginterp, wdwarf, log g, radii.
 //   k_phase    : one thread per datum: ephemeris + Roemer phase and the
 //                exposure sub-divisions (orchestration.rs:231-241,
 //                flux.rs:379-387) with their earth vectors.
+//   k_elements : one thread per grid element of every model in the batch.
+//                Surface point (surface.rs:54-121) or sphere point, area,
+//                gravity (grid.rs:201-322; disc/rim/spot grid.rs:336-553);
+//                eclipse intervals by a spherical star (eclipse.rs:229-265)
+//                and by an opaque disc (disc_eclipse.rs:84-330); continuum
+//                flux (brightness.rs).  Elements eclipsed by a Roche-distorted
+//                star keep that slot for k_roche.
+//   k_roche    : one thread per element eclipsed by a Roche-distorted star:
+//                the FP64 ray-march ingress_egress (eclipse.rs:270-373), the
+//                phase scan with exact lower-bound miss proofs, then the two
+//                bisections.  Small batches run k_roche_scan (the scan split
+//                over several threads, first hit by atomicMin) and
+//                k_roche_chop (the bisections from that hit) instead.
+//   k_aux      : per star element, the per-model FP64 sums of ginterp,
+//                wdwarf, log g and radii (flux.rs:115-206, 288-373).
 //   k_flux     : persistent FP32 flux sum (flux.rs:7-111) over work units of
 //                (element range x 512 sub-phases).  Element chunks arrive in
-//                shared memory by cp.async.bulk (TMA) double buffering; each
-//                thread keeps 4 sub-phases in registers and accumulates in
-//                FP32 blocks of 32 elements folded into a two-sum pair.
+//                shared memory by cp.async.bulk (TMA) double buffering; a
+//                classification pass lists each chunk's contributing
+//                elements; each thread keeps 4 sub-phases in registers, in
+//                pairs on the packed FP32x2 pipe, and accumulates in FP32
+//                blocks of 32 elements folded into a two-sum pair.
 //                Visibility is decided exactly in FP64 per (element, tile)
 //                and per sub-phase only where an eclipse edge falls inside
 //                the tile.
 //   k_epilogue : one block per model: ginterp scale factors, exposure
 //                smearing, slope/third, chi-squared / re_scale
-//                (orchestration.rs:243-310, 361-401).
+//                (orchestration.rs:243-310, 361-401), and with iscale = 1 the
+//                per-component fluxes and their one-sided Jacobi SVD scale
+//                factors (405-436).
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
