@@ -1,9 +1,12 @@
 // lcb_engine.cu — context, device buffers, batch execution and the C ABI.
 //
 // A batch runs as one launch sequence on the context's stream:
-//   memset(aux, status, counter) -> k_phase -> k_elements -> k_flux -> k_epilogue
+//   memset(aux, status, counter) -> k_phase -> k_elements -> k_roche (or, for
+//   small batches, k_roche_scan -> k_roche_chop) -> k_aux -> k_flux -> k_epilogue
 // For a resident batch (lcb_batch_*) the sequence is captured once in a CUDA
-// graph and replayed; only the model table changes between runs.
+// graph and replayed; between runs only the model table and the tables
+// derived from it are uploaded, and the graph is rebuilt only when the
+// plan's shapes change.
 #include <cuda_runtime.h>
 
 #include <algorithm>
