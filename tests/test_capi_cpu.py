@@ -22,6 +22,31 @@ def test_library_exports_every_declared_symbol(lcb):
     assert set(syms) == set(lcb._capi.SYMBOLS)
 
 
+def header_prototypes():
+    """name -> (return type, parameter count) of every lcb_* prototype in include/*.h."""
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"(const\s+char\s*\*|void|int)\s+(lcb_[a-z_0-9]+)\s*\(([^;{]*?)\)\s*;", text):
+        params = " ".join(m.group(3).split())
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        out[m.group(2)] = (" ".join(m.group(1).split()), n)
+    return out
+
+
+def test_ctypes_signatures_match_the_headers(lcb):
+    """Every declared function has as many ctypes argument types as the C
+    prototype has parameters, and the matching return type."""
+    L = lcb._capi.load()
+    protos = header_prototypes()
+    assert set(protos) == set(header_symbols())
+    want_res = {"int": C.c_int, "void": None, "const char *": C.c_char_p, "const char*": C.c_char_p}
+    for name, (ret, n) in protos.items():
+        f = getattr(L, name)
+        assert f.argtypes is not None and len(f.argtypes) == n, (name, n, f.argtypes)
+        assert f.restype is want_res[ret], (name, ret, f.restype)
+
+
 def test_version_and_errors(lcb):
     L = lcb._capi.load()
     assert b"sm_100a" in L.lcb_version()
