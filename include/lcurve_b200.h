@@ -189,6 +189,17 @@ int  lcb_batch_stats(const lcb_batch* b, int64_t* out8);
  * miss by the lower bound and skipped].  The line-of-sight searches are
  * exactly the reference path's (eclipse.rs:123-197 calls). */
 int  lcb_batch_search_counts(const lcb_batch* b, int64_t* out5);
+/* Launch-shape choices of a resident batch, for an autotuner (no reference
+ * counterpart; the reference GPU crate launches one fixed shape, 256-thread
+ * blocks, crates/lcurve-cuda/kernels/flux_kernel.cu:81, 543-545): elements
+ * per flux work unit in chunks of 256 (1..16), threads per Roche-eclipsed
+ * element in the phase scan (1..16; only where the batch has such elements)
+ * and persistent flux blocks per SM (>= 1, capped at the occupancy limit);
+ * 0 keeps the planner's heuristic for that choice.  Re-plans the batch;
+ * results are unchanged up to the FP32 summation order of the flux sum.
+ * lcb_batch_get_tuning reports the three values in effect. */
+int  lcb_batch_set_tuning(lcb_batch* b, int flux_chunks, int roche_split, int flux_blocks_per_sm);
+int  lcb_batch_get_tuning(const lcb_batch* b, int* out3);
 /* Same evaluation as lcb_batch_run but issued as direct launches with CUDA
  * events between the stages (events recorded inside a graph carry no timing),
  * for per-kernel device times. */

@@ -365,6 +365,16 @@ class Batch:
     def run(self, scale=False) -> None:
         check(_capi.load().lcb_batch_run(self._h, int(bool(scale))))
 
+    def set_tuning(self, flux_chunks: int = 0, roche_split: int = 0, flux_blocks_per_sm: int = 0) -> None:
+        """Launch-shape choices (lcb_batch_set_tuning); 0 = the planner's heuristic."""
+        check(_capi.load().lcb_batch_set_tuning(self._h, int(flux_chunks), int(roche_split), int(flux_blocks_per_sm)))
+
+    def tuning(self) -> dict:
+        """The launch-shape choices in effect (lcb_batch_get_tuning)."""
+        a = (C.c_int * 3)()
+        check(_capi.load().lcb_batch_get_tuning(self._h, a))
+        return dict(flux_chunks=a[0], roche_split=a[1], flux_blocks_per_sm=a[2])
+
     def search_counts(self) -> dict:
         a = np.zeros(5, dtype=np.int64)
         check(_capi.load().lcb_batch_search_counts(self._h, i64ptr(a)))

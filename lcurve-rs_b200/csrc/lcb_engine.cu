@@ -102,6 +102,7 @@ struct lcb_batch {
     std::vector<int64_t> start, count;
     lcb::Plan plan;
     lcb::Plan spare;  // the plan before the last lcb_batch_set_params: its storage is planned into next
+    lcb::PlanTuning tune;  // launch-shape choices (lcb_batch_set_tuning); zeros = heuristics
     DeviceSet dev;
     cudaGraphExec_t graph = nullptr;
     int graph_scale = -1;
@@ -204,7 +205,9 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
                      D.counter.as<int>(), D.rec.as<float4>(), D.pos.as<float4>(), D.ecl.as<double2>(),
                      D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
                      D.status.as<int>()};
-    int64_t grid = (int64_t)C->num_sms * lcb::flux_blocks_per_sm();
+    const int bps_max = lcb::flux_blocks_per_sm();
+    const int bps = P.flux_blocks_per_sm > 0 ? std::min(P.flux_blocks_per_sm, bps_max) : bps_max;
+    int64_t grid = (int64_t)C->num_sms * bps;
     grid = std::min<int64_t>(grid, std::max<int64_t>((int64_t)P.units.size(), 1));
     CUDA_TRY(lcb::launch_flux(fa, (int)grid, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[5], s));
@@ -590,7 +593,8 @@ int lcb_batch_create(lcb_ctx* C, const lcb_model* const* models, int64_t nmodels
         }
         std::vector<const lcb::Model*> mp(nmodels);
         for (int64_t i = 0; i < nmodels; ++i) mp[i] = &B->models[i];
-        lcb::plan_batch(mp.data(), nmodels, B->data.data(), B->start.data(), B->count.data(), C->num_sms, B->plan);
+        lcb::plan_batch(mp.data(), nmodels, B->data.data(), B->start.data(), B->count.data(), C->num_sms, B->plan,
+                        B->tune);
         upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), true);
         CUDA_TRY(cudaStreamSynchronize(C->stream));
     });
@@ -612,6 +616,49 @@ void lcb_batch_destroy(lcb_batch* B) {
     delete B;
 }
 
+// Re-plans a resident batch after its models or its tuning changed: plans into the spare
+// storage, uploads what changed, drops the captured graph when the shapes changed.
+static void replan_batch(lcb_batch* B) {
+    lcb_ctx* C = B->ctx;
+    const int64_t n = (int64_t)B->models.size();
+    std::vector<const lcb::Model*> mp(n);
+    for (int64_t i = 0; i < n; ++i) mp[i] = &B->models[i];
+    lcb::Plan& P = B->spare;
+    lcb::plan_batch(mp.data(), n, B->data.data(), B->start.data(), B->count.data(), C->num_sms, P, B->tune);
+    const bool same = P.shape_key == B->plan.shape_key;
+    std::swap(B->plan, P);
+    upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
+    if (!same && B->graph) {
+        cudaGraphExecDestroy(B->graph);
+        B->graph = nullptr;
+    }
+    CUDA_TRY(cudaStreamSynchronize(C->stream));
+}
+
+int lcb_batch_set_tuning(lcb_batch* B, int flux_chunks, int roche_split, int flux_blocks_per_sm) {
+    if (!B) return fail(LCB_ERR_INVALID, "null batch");
+    if (flux_chunks < 0 || flux_chunks > 16 || roche_split < 0 || roche_split > 16 || flux_blocks_per_sm < 0)
+        return fail(LCB_ERR_INVALID, "tuning out of range (flux_chunks, roche_split 0..16; blocks per SM >= 0)");
+    lcb_ctx* C = B->ctx;
+    return guarded(C, [&] {
+        B->tune.flux_chunks = flux_chunks;
+        B->tune.roche_split = roche_split;
+        B->tune.flux_blocks_per_sm = flux_blocks_per_sm;
+        replan_batch(B);
+    });
+}
+
+int lcb_batch_get_tuning(const lcb_batch* B, int* out3) {
+    if (!B || !out3) return fail(LCB_ERR_INVALID, "null pointer");
+    return guarded(B->ctx, [&] {
+        const lcb::Plan& P = B->plan;
+        const int bps_max = lcb::flux_blocks_per_sm();
+        out3[0] = P.flux_chunks;
+        out3[1] = P.roche_split;
+        out3[2] = P.flux_blocks_per_sm > 0 ? std::min(P.flux_blocks_per_sm, bps_max) : bps_max;
+    });
+}
+
 int lcb_batch_set_params(lcb_batch* B, const char* const* names, int ndim, const double* values) {
     if (!B || !names || !values || ndim <= 0) return fail(LCB_ERR_INVALID, "bad arguments");
     lcb_ctx* C = B->ctx;
@@ -622,21 +669,10 @@ int lcb_batch_set_params(lcb_batch* B, const char* const* names, int ndim, const
             if (k < 0) throw Error(LCB_ERR_UNKNOWN_PARAM, std::string("unknown parameter: '") + names[j] + "'");
             for (int64_t i = 0; i < n; ++i) B->models[i].p[k].value = values[i * ndim + j];
         }
-        std::vector<const lcb::Model*> mp(n);
-        for (int64_t i = 0; i < n; ++i) mp[i] = &B->models[i];
-        // plan into the previous call's storage (kept capacity: no allocation or first-touch page
-        // faults when a resident batch is re-parameterised step after step)
-        lcb::Plan& P = B->spare;
-        lcb::plan_batch(mp.data(), n, B->data.data(), B->start.data(), B->count.data(), C->num_sms, P);
-        const bool same = P.shape_key == B->plan.shape_key;
-        std::swap(B->plan, P);
-        // unchanged shapes: only the model table and the tables derived from it change
-        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
-        if (!same && B->graph) {
-            cudaGraphExecDestroy(B->graph);
-            B->graph = nullptr;
-        }
-        CUDA_TRY(cudaStreamSynchronize(C->stream));
+        // planned into the previous call's storage (kept capacity: no allocation or first-touch
+        // page faults when a resident batch is re-parameterised step after step); with unchanged
+        // shapes only the model table and the tables derived from it are uploaded
+        replan_batch(B);
     });
 }
 

@@ -744,7 +744,7 @@ void parallel_for(int64_t n, int64_t grain, F&& f) {
 }
 
 void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, const int64_t* start,
-                const int64_t* count, int num_sms, Plan& P) {
+                const int64_t* count, int num_sms, Plan& P, const PlanTuning& tune) {
     P.reset();
     P.models.resize(n);
     P.model_ok.assign(n, 0);
@@ -880,6 +880,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         const int64_t threads = (int64_t)P.rblocks.size() * kRocheBlock;
         const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 4;
         P.roche_split = threads > 0 ? (int)std::min<int64_t>(std::max<int64_t>(target / threads, 1), 16) : 1;
+        if (tune.roche_split > 0 && threads > 0) P.roche_split = std::min(std::max(tune.roche_split, 1), 16);
     }
 
     // flux work units: choose the element range so there are a few units per resident block
@@ -891,6 +892,9 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     int64_t erange = per_unit / kFluxTile;
     erange = std::min<int64_t>(std::max<int64_t>(erange, kFluxChunk), 16 * kFluxChunk);
     erange = (erange + kFluxChunk - 1) / kFluxChunk * kFluxChunk;
+    if (tune.flux_chunks > 0) erange = (int64_t)std::min(std::max(tune.flux_chunks, 1), 16) * kFluxChunk;
+    P.flux_chunks = (int)(erange / kFluxChunk);
+    P.flux_blocks_per_sm = std::max(tune.flux_blocks_per_sm, 0);
 
     thread_local std::vector<std::pair<int64_t, FluxUnit>> fu;  // scratch kept across calls
     fu.clear();
@@ -984,7 +988,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     // shape key: what the device buffers and the captured graph depend on
     P.shape_key = {n, P.nelem, P.nsub, P.ndatum, P.npartial, (int64_t)P.units.size(), (int64_t)P.eblocks.size(),
                    (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(), (int64_t)P.segs.size(),
-                   (int64_t)P.bands.size(), (int64_t)P.rings.size(), (int64_t)P.roche_split};
+                   (int64_t)P.bands.size(), (int64_t)P.rings.size(), (int64_t)P.roche_split,
+                   (int64_t)P.flux_blocks_per_sm};
 }
 
 }  // namespace lcb

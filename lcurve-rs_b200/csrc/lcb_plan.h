@@ -9,6 +9,14 @@
 
 namespace lcb {
 
+// Launch-shape choices an autotuner may fix; 0 leaves each to the planner's heuristic.  Every
+// value lies in the range the heuristic itself produces, so the kernels handle it as usual.
+struct PlanTuning {
+    int flux_chunks = 0;         // elements per flux work unit, in chunks of kFluxChunk (1..16)
+    int roche_split = 0;         // threads per Roche-eclipsed element in the phase scan (1..16)
+    int flux_blocks_per_sm = 0;  // persistent flux blocks per SM (1..occupancy limit)
+};
+
 struct Plan {
     std::vector<ModelDev> models;
     std::vector<SegDesc> segs;
@@ -31,6 +39,8 @@ struct Plan {
     bool datum_contiguous = false;
     bool any_iscale = false;  // some model fits per-component scale factors (needs fcomp scratch)
     int roche_split = 1;      // threads per Roche-eclipsed element in the phase scan
+    int flux_chunks = 1;      // elements per flux work unit / kFluxChunk
+    int flux_blocks_per_sm = 0;  // persistent flux blocks per SM; 0 = the occupancy limit
 
     // Empties the plan but keeps every buffer's capacity, so re-planning a
     // batch of the same size touches no fresh memory.
@@ -42,6 +52,8 @@ struct Plan {
         datum_contiguous = false;
         any_iscale = false;
         roche_split = 1;
+        flux_chunks = 1;
+        flux_blocks_per_sm = 0;
     }
 };
 
@@ -49,7 +61,7 @@ struct Plan {
 // (ranges may overlap, e.g. one shared data set).  Models that are physically
 // invalid are marked failed (model_ok = 0) instead of throwing.
 void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, const int64_t* start,
-                const int64_t* count, int num_sms, Plan& out);
+                const int64_t* count, int num_sms, Plan& out, const PlanTuning& tune = PlanTuning{});
 
 // Host FP64 helpers also used by tests of the planner.
 double host_xl1(double q);

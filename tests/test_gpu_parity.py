@@ -217,3 +217,42 @@ def test_time_split_light_curve_through_nccl_matches_light_curve(lcb):
         assert np.allclose(r.calc, ref.calc, rtol=1e-12, atol=0)
         assert np.isclose(r.chisq, ref.chisq, rtol=1e-12) and r.wnok == ref.wnok
         assert np.isclose(r.wdwarf, ref.wdwarf, rtol=1e-12) and np.allclose(r.sfac, ref.sfac, rtol=1e-12)
+
+
+def test_batch_tuning_keeps_results(lcb, W):
+    """lcb_batch_set_tuning: every launch-shape choice an autotuner may set
+    gives the default plan's fluxes and chi-squared, up to the FP32 summation
+    order of the flux sum (fluxes 1e-6 relative, ten times inside the oracle
+    bound; chi-squared 1e-4, which magnifies a flux change by about flux /
+    noise = 100), and lcb_batch_get_tuning reports what was set; zeros
+    restore the heuristic."""
+    specs = W.batch_models(n=6, seed=5, nlat1=(20, 40), nlat2=(30, 60), ntime=(150, 300))
+    models = [lcb.Model(text=s) for s, _ in specs]
+    fid = lcb.Model(text=W.single_small()[0])
+    datas, offs = [], [0]
+    for i, (_, t) in enumerate(specs):
+        f = fid.light_curve(times=t, expose=0.001, ndiv=1).flux
+        datas.append(W.noisy_data(t, f, 0.001, 1, seed=100 + i))
+        offs.append(offs[-1] + len(t))
+    data = np.concatenate(datas)
+    B = lcb.Batch(models, data, offs)
+    B.run(scale=True)
+    chi0, calc0, _ = B.results(want_calc=True)
+    heuristic = B.tuning()
+    assert B.stats()["roche_elements"] > 0
+    for tune in ((1, 1, 1), (16, 16, 2), (4, 3, 0), (0, 8, 1)):
+        B.set_tuning(*tune)
+        got = B.tuning()
+        if tune[0]:
+            assert got["flux_chunks"] == tune[0]
+        if tune[1]:
+            assert got["roche_split"] == tune[1]
+        assert got["flux_blocks_per_sm"] == (min(tune[2], heuristic["flux_blocks_per_sm"]) if tune[2]
+                                             else heuristic["flux_blocks_per_sm"])
+        for _ in range(2):  # the captured graph, then its replay
+            B.run(scale=True)
+            chi, calc, _ = B.results(want_calc=True)
+            assert np.allclose(calc, calc0, rtol=1e-6, atol=0), tune
+            assert np.allclose(chi, chi0, rtol=1e-4, atol=0), tune
+    B.set_tuning(0, 0, 0)
+    assert B.tuning() == heuristic

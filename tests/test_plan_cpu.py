@@ -26,6 +26,7 @@ from conftest import GOLDEN, ROOT
 DRIVER = r"""
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -55,8 +56,13 @@ int main(int argc, char** argv) {
             d.ndiv = (k + (int)i) % 4 == 0 ? 3 : 1; data.push_back(d);
         }
     }
+    PlanTuning tune;
+    if (argc > 4) { tune.flux_chunks = std::atoi(argv[2]); tune.roche_split = std::atoi(argv[3]); tune.flux_blocks_per_sm = std::atoi(argv[4]); }
     Plan P;
-    plan_batch(mp.data(), n, data.data(), st.data(), cnt.data(), 148, P);
+    plan_batch(mp.data(), n, data.data(), st.data(), cnt.data(), 148, P, tune);
+    if (tune.flux_chunks > 0) CHECK(P.flux_chunks == tune.flux_chunks, "flux_chunks %d", P.flux_chunks);
+    if (tune.roche_split > 0 && P.roche_elems > 0) CHECK(P.roche_split == tune.roche_split, "roche_split %d", P.roche_split);
+    CHECK(P.flux_blocks_per_sm == tune.flux_blocks_per_sm, "flux_blocks_per_sm");
     // segments: contiguous per model, in order
     int64_t e = 0;
     std::vector<int64_t> mfirst(n, -1), mcount(n, 0);
@@ -139,7 +145,7 @@ int main(int argc, char** argv) {
         if (!P.model_ok[i]) { ++failed; CHECK(mcount[i] == 0 && !P.model_err[i].empty(), "failed model %lld", (long long)i); }
     // re-planning into the same storage
     Plan Q = P;
-    plan_batch(mp.data(), n, data.data(), st.data(), cnt.data(), 148, P);
+    plan_batch(mp.data(), n, data.data(), st.data(), cnt.data(), 148, P, tune);
     CHECK(same(P.segs, Q.segs) && same(P.bands, Q.bands) && same(P.rings, Q.rings) && same(P.units, Q.units) &&
           same(P.eblocks, Q.eblocks) && same(P.rblocks, Q.rblocks) && same(P.ablocks, Q.ablocks) &&
           same(P.models, Q.models) && same(P.datum_sub0, Q.datum_sub0) && P.shape_key == Q.shape_key,
@@ -186,6 +192,11 @@ def test_plan_invariants(driver):
     r = subprocess.run([str(driver / "d"), str(driver / "models.bin")], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "failed 1 " in r.stdout, r.stdout
+    # the same invariants under every launch-shape choice an autotuner may set
+    for tune in ((1, 1, 1), (16, 16, 4), (4, 2, 0), (2, 0, 3)):
+        r = subprocess.run([str(driver / "d"), str(driver / "models.bin")] + [str(v) for v in tune],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, (tune, r.stdout + r.stderr)
 
 
 HELPERS = r"""
