@@ -21,6 +21,9 @@ data (lcurve-rs_b200/workloads.py).
           Defaults are a reduced run (524k curves, 3000 steps); --mcmc-full
           runs the full 1M-curve, 20000-step configuration.
 
+  --autotune : tune the resident batch's launch shapes before timing (the
+          default run uses the planner's heuristics).
+
   --train-profile K : only the surrogate's training step (8192 curves), K
           steps after --warmup, one JSON line (the profiling entry point).
 
@@ -72,6 +75,8 @@ def parse():
     p.add_argument("--mcmc-burn", type=int, default=500)
     p.add_argument("--mcmc-substeps", type=int, default=2)
     p.add_argument("--mcmc-bandwidth", type=float, default=0.6, help="KDE bandwidth in units of Scott's factor")
+    p.add_argument("--autotune", action="store_true",
+                   help="tune the resident batch's launch shapes (lcurve-rs_b200/autotune.py) before timing")
     p.add_argument("--train-profile", type=int, default=0, metavar="K",
                    help="time K surrogate training steps (8192 curves) alone, print one JSON line and exit")
     a = p.parse_args()
@@ -362,6 +367,9 @@ def main():
 
     specs, models, data, offs = build_workload(lcb, W, args.models, 1234 + rank)
     B = lcb.Batch(models, data, offs)
+    tuned = None
+    if args.autotune:  # off by default: the heuristics' launch shapes
+        tuned = importlib.import_module("lcurve-rs_b200.autotune").autotune(B, scale=False, repeats=1)
     st = B.stats()
     for _ in range(args.warmup):
         B.run(scale=False)
@@ -409,7 +417,8 @@ def main():
         wall = (time.perf_counter() - w0) / args.steps * 1e3
         h2d, d2h = lcb.transfer_bytes()
         e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall), "cuda")
-        same = bool(np.allclose(c2, chi, rtol=1e-9, equal_nan=True))
+        # a tuned batch differs from the transient (heuristic) plan in FP32 summation order only
+        same = bool(np.allclose(c2, chi, rtol=1e-4 if tuned else 1e-9, equal_nan=True))
         e2e = {"value": weak_value(world, args.models, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "matches_resident": same}
 
@@ -462,6 +471,7 @@ def main():
                    "subphases_per_step": st["subphases"], "element_evals_per_step": st["element_evals"],
                    "roche_eclipsed_elements": st["roche_elements"], "roche_search": counts,
                    "flux_units": st["flux_units"],
+                   **({"autotuned": tuned} if tuned else {}),
                    "stage_ms": dict(zip(stage_names, [float(x) for x in stage])),
                    "l2": "inputs larger than L2 (element arrays > 10 GB per step)",
                    "parallelism": f"weak, {world} independent batches"},
