@@ -146,25 +146,60 @@ def build_workload(lcb, W, n, seed):
     fid = [lcb.Model(text=fid_text) for _ in range(n)]
     tmpl = lcb.make_data(times, expose=0.001, ndiv=1, flux=1.0, ferr=1.0, weight=1.0)
     _, fflux, _ = lcb.chisq_batch_ragged(fid, tmpl, offs, scale=False, want_calc=True)
-    rng = np.random.default_rng(seed + 99)
-    sig = 0.01 * np.abs(fflux)
-    data = lcb.make_data(times, expose=0.001, ndiv=1, flux=fflux + sig * rng.standard_normal(fflux.shape),
-                         ferr=sig, weight=1.0)
+    flux, sig = W.batch_noise(fflux, seed)
+    data = lcb.make_data(times, expose=0.001, ndiv=1, flux=flux, ferr=sig, weight=1.0)
     return specs, models, data, offs
 
 
-def cpu_models_per_s(specs, data, offs, first, count, nthreads):
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def cpu_sample(specs, data, offs, sel, nthreads):
+    """The oracle's chi-squared of the models `sel` on all host threads, with
+    the reference's Rayon loops (models, and within each model its times, in
+    parallel; threads that run out of models help with other models' times).
+    Returns (chisq, wall-clock models/s, steady-state models/s).  Steady state
+    is the rate of a batch long enough to keep every thread busy, as the
+    reference's chisq_batch over 1024 models is: models x threads / process
+    CPU seconds.  A short sample's own wall clock undercounts it, since its
+    last models run while other threads idle."""
+    import resource
+
     from oracle import oracle as O
-    sel = [(first + k) % len(specs) for k in range(count)]
     oms = [O.Model(text=specs[i][0]) for i in sel]
     parts, o2 = [], [0]
     for i in sel:
         parts.append(data[offs[i]:offs[i + 1]])
         o2.append(o2[-1] + offs[i + 1] - offs[i])
     d = np.concatenate(parts)
+    r0 = resource.getrusage(resource.RUSAGE_SELF)
     t0 = time.perf_counter()
-    O.chisq_ragged(oms, d, o2, scale=False, nthreads=nthreads)
-    return count / (time.perf_counter() - t0)
+    chi = O.chisq_ragged(oms, d, o2, scale=False, nthreads=nthreads)
+    wall = time.perf_counter() - t0
+    r1 = resource.getrusage(resource.RUSAGE_SELF)
+    cpu = (r1.ru_utime - r0.ru_utime) + (r1.ru_stime - r0.ru_stime)
+    return chi, len(sel) / wall, len(sel) * nthreads / max(cpu, 1e-9)
+
+
+def cpu_description(nthreads) -> dict:
+    from oracle import oracle as O
+    return {"cores": nthreads, "cpu_model": O.host_cpu(),
+            "build": "oracle/lcurve_oracle.cpp, g++ -O3 -march=native -ffp-contract=off, built on this host"}
+
+
+def bench_golden(models: int, seed: int):
+    """Committed oracle answers for this batch (tests/golden/make_bench_golden.py), if any."""
+    p = ROOT / "tests" / "golden" / f"batch_{models}_seed{seed}.json"
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text())
+    except (ValueError, OSError):
+        return None
 
 
 def traffic_from_profiles(kernel):
@@ -179,34 +214,55 @@ def traffic_from_profiles(kernel):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU path (the oracle, the FP64 restatement of the
+    reference's Rayon chisq_batch, built for this host's CPU) on the same
+    1024-model batch and data.  Each timed step evaluates 2 x threads models,
+    rotating through the batch; warm-up steps a few."""
     if rank != 0:
         return
     W = importlib.import_module("lcurve-rs_b200.workloads")
-    from oracle import oracle as O  # noqa: F401  (builds/loads the oracle)
-    nthreads = os.cpu_count() or 1
-    sample = args.cpu_sample or nthreads
+    from oracle import oracle as O
+    O.use_native()
+    nthreads = host_threads()
+    sample = args.cpu_sample or 2 * nthreads
+    warm = max(1, nthreads // 4)
     specs = W.batch_models(n=args.models, seed=1234)
-    offs = np.zeros(len(specs) + 1, dtype=np.int64)
+    n = len(specs)
+    offs = np.zeros(n + 1, dtype=np.int64)
     offs[1:] = np.cumsum([len(t) for _, t in specs])
     times = np.concatenate([t for _, t in specs])
-    # chi-squared needs data; its values do not change the work
-    data = O.make_data(times, expose=0.001, ndiv=1, flux=1.0, ferr=0.01, weight=1.0)
-    rates = []
-    for s in range(args.warmup + args.steps):
-        r = cpu_models_per_s(specs, data, offs, s * sample, sample, nthreads)
+    # the b200 arm's data: the single_small curve at every model's times + 1% noise; the
+    # curve is evaluated (by the CPU path) only where a sampled model needs it
+    sels = [[(s * warm + k) % n for k in range(warm)] for s in range(args.warmup)]
+    sels += [[(s * sample + k) % n for k in range(sample)] for s in range(args.steps)]
+    need = np.zeros(times.shape[0], dtype=bool)
+    for i in {i for sel in sels for i in sel}:
+        need[offs[i]:offs[i + 1]] = True
+    fid = np.zeros(times.shape[0])
+    fid[need] = O.Model(text=W.single_small()[0]).light_curve(O.make_data(times[need]), nthreads=nthreads)["calc"]
+    flux, sig = W.batch_noise(fid, 1234)
+    data = O.make_data(times, expose=0.001, ndiv=1, flux=flux, ferr=sig, weight=1.0)
+    steady, wall = [], []
+    for s, sel in enumerate(sels):
+        _, rw, rs = cpu_sample(specs, data, offs, sel, nthreads)
         if s >= args.warmup:
-            rates.append(r)
-    v = float(np.mean(rates))
+            wall.append(rw)
+            steady.append(rs)
+    v = float(np.mean(steady))
+    cpu = cpu_description(nthreads)
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sample / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"batch_{args.models}: uneven models (nlat1f U{{30..300}}, nlat2f U{{30..500}}, "
-                               f"ntime U{{200..5000}}), seed 1234", "sample_models_per_step": sample},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
-                         "sample": f"{sample} models per step of the 1024-model batch, all host threads "
-                                   "(oracle/lcurve_oracle.cpp, parallel over models as the reference's Rayon "
-                                   "chisq_batch)"},
+                               f"ntime U{{200..5000}}, q/iangle/r1/t1/t2 uniform), seed 1234",
+                   "sample_models_per_step": sample, "warmup_models_per_step": warm,
+                   "wall_clock_models_per_s": float(np.mean(wall))},
+        "cpu_baseline": {"value": v, "unit": UNIT, "kind": "port", **cpu,
+                         "sample": f"{sample} models per step rotating through the 1024-model batch "
+                                   f"({args.steps * sample} models), all host threads, nested model/time "
+                                   "parallelism as the reference's Rayon chisq_batch; value = steady-state rate "
+                                   "(models x threads / process CPU s), wall-clock rate in config"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "mcmc": {"skipped": "the MCMC comparison runs the GPU engine and surrogate; the reference arm times "
                             "the CPU light-curve path only"},
@@ -427,35 +483,64 @@ def main():
             dist.destroy_process_group()
         return
 
+    # ---- parity of this run's batch against the oracle's committed answers (all models)
+    golden = bench_golden(args.models, 1234 + rank)
+    parity = {}
+    if golden is not None:
+        if W.workload_key(specs) == golden["workload_sha1"]:
+            ref = np.asarray(golden["chisq"])
+            parity["batch_vs_oracle"] = {
+                "models": int(ref.size), "max_rel_err_chisq": float(np.max(np.abs(chi - ref) / np.abs(ref))),
+                "searches": int(counts["searches"]), "oracle_searches": int(golden["counters"]["fblink"]),
+                "source": "tests/golden/batch_1024_seed1234.json (oracle, tests/golden/make_bench_golden.py)"}
+
     # ---- roofline of the dominant kernel
     p64 = lcb.fma_peak_tflops(True)
     p32 = lcb.fma_peak_tflops(False)
-    # FP64 work of the Roche search as executed: potential and gradient evaluations plus
-    # lower-bound nodes (each costs about one potential evaluation)
+    # FP64 work of the Roche search, two ways: as executed on the device (potential and
+    # gradient evaluations plus lower-bound nodes, each about one potential evaluation),
+    # and as the reference's algorithm counts it (the oracle's potential and gradient
+    # evaluations for this batch; the device proves most misses without them)
     roche_flops = (counts["pot_evals"] + counts["dpot_evals"] + counts["bound_nodes"]) * POT_FLOPS_PER_EVAL
+    roche_alg = None
+    if golden is not None and parity:
+        roche_alg = (golden["counters"]["rpot"] + golden["counters"]["drpot"]) * POT_FLOPS_PER_EVAL
     flux_flops = st["element_evals"] * FLUX_FLOPS_PER_EVAL
     kernels = {
-        "k_roche": {"ms": stage[2], "flops": roche_flops, "peak": p64, "pipe": "fp64"},
-        "k_flux": {"ms": stage[4], "flops": flux_flops, "peak": p32, "pipe": "fp32"},
+        "k_roche": {"ms": stage[2], "flops": roche_alg or roche_flops, "peak": p64, "pipe": "fp64",
+                    "work": "reference-algorithm potential evaluations (oracle count) x 22" if roche_alg
+                    else "executed potential/gradient/bound evaluations x 22"},
+        "k_flux": {"ms": stage[4], "flops": flux_flops, "peak": p32, "pipe": "fp32",
+                   "work": "element-evals x 17"},
     }
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     k = kernels[dom]
     ach = k["flops"] / (k["ms"] / 1e3) / 1e12
+    tf = lambda fl, ms: fl / (ms / 1e3) / 1e12 if ms else None  # noqa: E731
     roof = {"kernel": dom, "bound": k["pipe"], "achieved": ach, "peak": k["peak"], "unit": "TFLOP/s",
             "frac": ach / k["peak"] if k["peak"] else None, "traffic": traffic_from_profiles(dom),
+            "work": k["work"],
             "peak_source": f"measured {k['pipe'].upper()} FMA peak of this GPU (k_fma_peak); "
-                           "MEASURED_PEAKS.json has HBM and bf16 only",
-            "other": {n: {"ms": v["ms"], "achieved_tflops": v["flops"] / (v["ms"] / 1e3) / 1e12 if v["ms"] else None,
-                          "peak_tflops": v["peak"]} for n, v in kernels.items()}}
+                           "MEASURED_PEAKS.json has no FP32/FP64 figure",
+            "k_roche_executed": {"achieved_tflops": tf(roche_flops, stage[2]),
+                                 "frac": tf(roche_flops, stage[2]) / p64 if stage[2] and p64 else None},
+            "other": {n: {"ms": v["ms"], "achieved_tflops": tf(v["flops"], v["ms"]), "peak_tflops": v["peak"],
+                          "work": v["work"]} for n, v in kernels.items()}}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        nthreads = os.cpu_count() or 1
-        sample = args.cpu_sample or nthreads
-        rate = cpu_models_per_s(specs, data, offs, 0, sample, nthreads)
-        cpu = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"first {sample} models of the batch, all host threads, parallel over models "
-                         "(oracle/lcurve_oracle.cpp, FP64 restatement of the reference CPU path)"}
+        from oracle import oracle as O
+        O.use_native()
+        nthreads = host_threads()
+        sample = args.cpu_sample or 2 * nthreads
+        sel = list(range(min(sample, len(specs))))
+        ochi, rate_wall, rate = cpu_sample(specs, data, offs, sel, nthreads)
+        cpu = {"value": rate, "unit": UNIT, "kind": "port", **cpu_description(nthreads),
+               "sample": f"first {len(sel)} models of the batch, all host threads, nested model/time parallelism "
+                         "as the reference's Rayon chisq_batch; value = steady-state rate (models x threads / "
+                         "process CPU s)", "wall_clock_models_per_s": rate_wall}
+        parity["sample_vs_oracle"] = {"models": len(sel),
+                                      "max_rel_err_chisq": float(np.max(np.abs(chi[sel] - ochi) / np.abs(ochi)))}
 
     mcmc = None
     if world == 1 and not args.no_mcmc:
@@ -476,6 +561,7 @@ def main():
                    "l2": "inputs larger than L2 (element arrays > 10 GB per step)",
                    "parallelism": f"weak, {world} independent batches"},
         "roofline": roof,
+        "parity": parity or None,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": 6 * args.steps,

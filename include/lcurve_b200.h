@@ -131,10 +131,11 @@ int lcb_light_curve(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data,
  * more scratch than the arena is rejected with LCB_ERR_INVALID and a message
  * giving the bytes needed (a grid element takes about 160 B, a datum about
  * 80 B, each exposure sub-division about 40 B plus 8 B per 4,096 elements).
- * The first call on a device looks up the arena's device address; make that
- * first call before any CUDA stream capture begins.  All calls on a device
- * share the arena: this library serialises them and waits for each call's GPU
- * work before returning, since calls whose GPU work overlapped would race. */
+ * Every call looks up the arena's device address on the context's device and
+ * waits for its own GPU work, so no call may be made while a CUDA stream
+ * capture is in progress on the calling thread.  All calls on a device share
+ * the arena: this library serialises them and waits for each call's GPU work
+ * before returning, since calls whose GPU work overlapped would race. */
 #define LCB_NOALLOC_ARENA_BYTES (64u * 1024u * 1024u)
 int lcb_light_curve_noalloc(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
                             int scale, int rdata, double* calc_out, lcb_result* res_out);
@@ -209,6 +210,30 @@ int  lcb_batch_profile(lcb_batch* b, int scale);
  * analytic eclipses), roche (FP64 ray-march), aux (per-model sums), flux,
  * epilogue]. */
 int  lcb_batch_stage_ms(const lcb_batch* b, double* out6);
+
+/* ---- work estimate (no reference counterpart) -------------------------------
+ * Host-only: plans one model on its data (no device work) and reports
+ * [grid elements, elements eclipsed by a Roche-distorted star, exposure
+ * sub-divisions, element-evaluations of the flux sum]; zeros for a model that
+ * is physically invalid.  Callers that split one batch over several devices
+ * (the reference's chisq_batch model loop, orchestration.rs:343-356) weigh
+ * models with it. */
+int lcb_model_work(const lcb_model* model, const lcb_datum* data, int64_t n, int64_t* out4);
+
+/* ---- failure-path hooks (no reference counterpart) ------------------------
+ * The eclipse search bounds one line-of-sight search at 262,144 potential
+ * evaluations (the reference's fblink, crates/roche/src/eclipse.rs:123-197,
+ * has no bound); a model whose search reaches it fails: NaN in the chisq_batch
+ * entry points (as the reference maps a failed model, orchestration.rs:
+ * 350-354) and LCB_ERR_DEVICE_CHECK from lcb_light_curve.
+ * lcb_ctx_set_search_cap lowers that bound for the context's later calls
+ * (0 restores the default), so the failure path can be exercised.
+ * lcb_wait_probe runs one block that waits on a barrier nothing completes,
+ * with the same bounded wait the flux kernel's copy pipeline uses, limited to
+ * limit_cycles SM cycles (<= 4e9); it returns LCB_ERR_DEVICE_CHECK when the
+ * wait gives up, as it must, and leaves the context usable. */
+int lcb_ctx_set_search_cap(lcb_ctx* ctx, int evals);
+int lcb_wait_probe(lcb_ctx* ctx, int64_t limit_cycles, int64_t* waited_cycles);
 
 /* ---- measurement utilities (no reference counterpart) --------------------
  * Bytes the last call on this context copied host->device / device->host. */

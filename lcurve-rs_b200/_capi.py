@@ -45,7 +45,8 @@ SYMBOLS = [
     "lcb_light_curve", "lcb_chisq_batch", "lcb_chisq_batch_ragged", "lcb_batch_create", "lcb_batch_destroy",
     "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_profile", "lcb_batch_stage_ms",
     "lcb_ctx_transfer_bytes", "lcb_measure_fma_peak", "lcb_model_grid", "lcb_batch_search_counts",
-    "lcb_light_curve_noalloc", "lcb_batch_set_tuning", "lcb_batch_get_tuning",
+    "lcb_light_curve_noalloc", "lcb_batch_set_tuning", "lcb_batch_get_tuning", "lcb_ctx_set_search_cap",
+    "lcb_wait_probe", "lcb_model_work",
     # surrogate (lcurve_b200_surrogate.h)
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
@@ -97,6 +98,9 @@ def load():
         "lcb_batch_set_tuning": ([vp, i, i, i], i),
         "lcb_batch_get_tuning": ([vp, C.POINTER(i)], i),
         "lcb_light_curve_noalloc": ([vp, vp, vp, i64, i, i, dp, C.POINTER(Result)], i),
+        "lcb_ctx_set_search_cap": ([vp, i], i),
+        "lcb_wait_probe": ([vp, i64, i64p], i),
+        "lcb_model_work": ([vp, vp, i64, i64p], i),
         "lcb_mlp_last_error": ([], cp),
         "lcb_mlp_create": ([i, i, i, i, i, i64, C.c_uint64, C.POINTER(vp)], i),
         "lcb_mlp_destroy": ([vp], None),

@@ -67,12 +67,16 @@ def autotune(batch, scale: bool = False, repeats: int = 2, cache: str | os.PathL
             ms = _device_time(batch, scale, repeats)
             if ms < best_ms:
                 best_ms, current = ms, batch.tuning()
-    batch.set_tuning(*(current[k] for k in KEYS))
+    # an axis that was not searched keeps the heuristic (0), so a cached choice applied to
+    # a batch that does have, say, Roche-eclipsed elements does not pin that axis
+    searched = {key for key, _ in axes}
+    choice = {k: (current[k] if k in searched else 0) for k in KEYS}
+    batch.set_tuning(*(choice[k] for k in KEYS))
     result = dict(current, ms=best_ms, heuristic_ms=heuristic_ms, **{"class": size_class(stats)})
     if cache is not None:
         path = pathlib.Path(cache)
         table = json.loads(path.read_text()) if path.exists() else {}
-        table.setdefault(device_name, {})[result["class"]] = {k: current[k] for k in KEYS}
+        table.setdefault(device_name, {})[result["class"]] = choice
         path.write_text(json.dumps(table, indent=1, sort_keys=True))
     return result
 

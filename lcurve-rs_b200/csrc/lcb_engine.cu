@@ -2,12 +2,13 @@
 //
 // A batch runs as one launch sequence on the context's stream:
 //   memset(aux, status, counter) -> k_phase -> k_elements -> k_roche (or, for
-//   small batches, k_roche_scan -> k_roche_chop) -> k_aux -> k_flux -> k_epilogue
+//   small batches, k_roche_scan -> k_roche_chop2) -> k_aux -> k_flux -> k_epilogue
 // For a resident batch (lcb_batch_*) the sequence is captured once in a CUDA
 // graph and replayed; between runs only the model table and the tables
 // derived from it are uploaded, and the graph is rebuilt only when the
 // plan's shapes change.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -32,6 +33,16 @@ int fail(int code, const std::string& msg) {
     t_last_error = msg;
     return code;
 }
+
+// NVTX range around one host-side stage (planning, uploads, launches, result
+// copies): visible in Nsight Systems / ncu's NVTX filters; header-only, inert
+// when no tool is attached.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 #define CUDA_TRY(expr)                                                                              \
     do {                                                                                            \
@@ -93,6 +104,8 @@ struct lcb_ctx {
     std::vector<lcb_datum> stage;  // host staging of gathered data
     cudaEvent_t ev[kStages + 1] = {};
     int64_t h2d = 0, d2h = 0;  // bytes moved by the current / last call
+    int fblink_cap = lcb::kFblinkEvalCap;  // lcb_ctx_set_search_cap
+    DevBuf probe;                          // lcb_wait_probe's status words
 };
 
 struct lcb_batch {
@@ -106,8 +119,10 @@ struct lcb_batch {
     DeviceSet dev;
     cudaGraphExec_t graph = nullptr;
     int graph_scale = -1;
+    int graph_cap = -1;  // the search cap baked into the captured graph's kernel arguments
     std::vector<int64_t> graph_key;
     bool ran = false;
+    bool broken = false;  // a re-plan failed part-way: buffers may not match the plan
     double stage_ms[kStages] = {0, 0, 0, 0, 0, 0};
     std::vector<double> h_results, h_calc;
     std::vector<int> h_status;
@@ -192,7 +207,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
                      D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
                      D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
                      (int64_t)P.eblocks.size(), (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(),
-                     D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>()};
+                     D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>(), C->fblink_cap};
     if (P.roche_split > 1)
         CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, P.rblocks.size() * lcb::kRocheBlock * sizeof(int), s));
     CUDA_TRY(lcb::launch_elements(ea, s));
@@ -251,10 +266,22 @@ void fill_result(const double* r, lcb_result* out) {
 void run_transient(lcb_ctx* C, const lcb::Model* const* models, int64_t n, const lcb_datum* data,
                    const int64_t* start, const int64_t* count, int scale, int rdata, std::vector<double>& res,
                    std::vector<double>* calc, lcb::Plan& P, std::vector<int>& st) {
-    lcb::plan_batch(models, n, data, start, count, C->num_sms, P);
-    upload_plan(C, C->scratch, P, data, 0, true);
-    enqueue_run(C, C->scratch, P, scale, rdata, false);
-    fetch_results(C, C->scratch, P, res, calc, &st);
+    {
+        Range r("lcb plan");
+        lcb::plan_batch(models, n, data, start, count, C->num_sms, P);
+    }
+    {
+        Range r("lcb upload");
+        upload_plan(C, C->scratch, P, data, 0, true);
+    }
+    {
+        Range r("lcb launch");
+        enqueue_run(C, C->scratch, P, scale, rdata, false);
+    }
+    {
+        Range r("lcb results");
+        fetch_results(C, C->scratch, P, res, calc, &st);
+    }
     for (int64_t i = 0; i < n; ++i)
         if (st[i] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
 }
@@ -333,6 +360,7 @@ void lcb_ctx_destroy(lcb_ctx* C) {
     cudaSetDevice(C->device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     C->scratch.release();
+    C->probe.release();
     for (auto& e : C->ev)
         if (e) cudaEventDestroy(e);
     if (C->own_stream && C->stream) cudaStreamDestroy(C->stream);
@@ -618,21 +646,41 @@ void lcb_batch_destroy(lcb_batch* B) {
 
 // Re-plans a resident batch after its models or its tuning changed: plans into the spare
 // storage, uploads what changed, drops the captured graph when the shapes changed.
+// If the uploads fail part-way (a buffer could not grow), the device buffers no longer
+// match the plan: the batch is marked broken, its graph dropped and its shape key
+// cleared, so no launch runs on it until a later re-plan uploads everything again.
 static void replan_batch(lcb_batch* B) {
     lcb_ctx* C = B->ctx;
     const int64_t n = (int64_t)B->models.size();
     std::vector<const lcb::Model*> mp(n);
     for (int64_t i = 0; i < n; ++i) mp[i] = &B->models[i];
     lcb::Plan& P = B->spare;
+    Range r("lcb replan");
     lcb::plan_batch(mp.data(), n, B->data.data(), B->start.data(), B->count.data(), C->num_sms, P, B->tune);
-    const bool same = P.shape_key == B->plan.shape_key;
+    const bool same = !B->broken && P.shape_key == B->plan.shape_key;
     std::swap(B->plan, P);
-    upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
-    if (!same && B->graph) {
-        cudaGraphExecDestroy(B->graph);
+    try {
+        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
+        if (!same && B->graph) {
+            cudaGraphExecDestroy(B->graph);
+            B->graph = nullptr;
+        }
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+    } catch (...) {
+        cudaStreamSynchronize(C->stream);
+        if (B->graph) cudaGraphExecDestroy(B->graph);
         B->graph = nullptr;
+        B->plan.shape_key.clear();
+        B->broken = true;
+        throw;
     }
-    CUDA_TRY(cudaStreamSynchronize(C->stream));
+    B->broken = false;
+}
+
+static void check_usable(const lcb_batch* B) {
+    if (B->broken)
+        throw Error(LCB_ERR_INVALID, "the batch's last re-plan failed (device memory); set its parameters or "
+                                     "tuning again before running it");
 }
 
 int lcb_batch_set_tuning(lcb_batch* B, int flux_chunks, int roche_split, int flux_blocks_per_sm) {
@@ -680,7 +728,8 @@ int lcb_batch_run(lcb_batch* B, int scale) {
     if (!B) return fail(LCB_ERR_INVALID, "null batch");
     lcb_ctx* C = B->ctx;
     return guarded(C, [&] {
-        if (B->graph && (B->graph_scale != scale || B->graph_key != B->plan.shape_key)) {
+        check_usable(B);
+        if (B->graph && (B->graph_scale != scale || B->graph_key != B->plan.shape_key || B->graph_cap != C->fblink_cap)) {
             cudaGraphExecDestroy(B->graph);
             B->graph = nullptr;
         }
@@ -701,7 +750,9 @@ int lcb_batch_run(lcb_batch* B, int scale) {
             CUDA_TRY(e);
             B->graph_scale = scale;
             B->graph_key = B->plan.shape_key;
+            B->graph_cap = C->fblink_cap;
         }
+        Range r("lcb batch run");
         CUDA_TRY(cudaGraphLaunch(B->graph, C->stream));
         fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
         CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
@@ -715,6 +766,7 @@ int lcb_batch_profile(lcb_batch* B, int scale) {
     if (!B) return fail(LCB_ERR_INVALID, "null batch");
     lcb_ctx* C = B->ctx;
     return guarded(C, [&] {
+        check_usable(B);
         enqueue_run(C, B->dev, B->plan, scale, 1, true);
         fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
         CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
@@ -734,6 +786,7 @@ int lcb_batch_results(lcb_batch* B, double* chisq_out, double* calc_out, lcb_res
     if (!B->ran) return fail(LCB_ERR_INVALID, "lcb_batch_run has not been called");
     lcb_ctx* C = B->ctx;
     return guarded(C, [&] {
+        check_usable(B);
         const lcb::Plan& P = B->plan;
         const int64_t n = (int64_t)P.models.size();
         for (int64_t i = 0; i < n; ++i) {
@@ -778,6 +831,41 @@ int lcb_ctx_transfer_bytes(const lcb_ctx* C, int64_t* h2d, int64_t* d2h) {
     return LCB_OK;
 }
 
+int lcb_model_work(const lcb_model* model, const lcb_datum* data, int64_t n, int64_t* out4) {
+    if (!model || (!data && n > 0) || !out4 || n < 0) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(nullptr, [&] {
+        const lcb::Model* mp = &model->m;
+        int64_t st = 0, cnt = n;
+        lcb::Plan P;
+        lcb::plan_batch(&mp, 1, data, &st, &cnt, 148, P);
+        const bool ok = !P.model_ok.empty() && P.model_ok[0];
+        int64_t v[4] = {ok ? P.nelem : 0, ok ? P.roche_elems : 0, ok ? P.nsub : 0, ok ? P.evals : 0};
+        std::memcpy(out4, v, sizeof v);
+    });
+}
+
+int lcb_ctx_set_search_cap(lcb_ctx* C, int evals) {
+    if (!C || evals < 0) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] { C->fblink_cap = evals > 0 ? evals : lcb::kFblinkEvalCap; });
+}
+
+int lcb_wait_probe(lcb_ctx* C, int64_t limit_cycles, int64_t* waited_cycles) {
+    if (!C || limit_cycles <= 0 || limit_cycles > 4000000000LL) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] {
+        C->probe.ensure(2 * sizeof(long long));
+        int* status = C->probe.as<int>();
+        long long* waited = C->probe.as<long long>() + 1;
+        CUDA_TRY(cudaMemsetAsync(C->probe.p, 0, 2 * sizeof(long long), C->stream));
+        CUDA_TRY(lcb::launch_wait_probe((long long)limit_cycles, status, waited, C->stream));
+        long long h[2] = {0, 0};
+        CUDA_TRY(cudaMemcpyAsync(h, C->probe.p, sizeof h, cudaMemcpyDeviceToHost, C->stream));
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+        if (waited_cycles) *waited_cycles = h[1];
+        if ((int)(h[0] & 0xffffffff) & lcb::kStatusTmaTimeout)
+            throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+    });
+}
+
 int lcb_measure_fma_peak(lcb_ctx* C, int which, double* tflops) {
     if (!C || !tflops || (which != 0 && which != 1)) return fail(LCB_ERR_INVALID, "bad arguments");
     return guarded(C, [&] { CUDA_TRY(lcb::measure_fma_peak(which, C->num_sms, C->stream, tflops)); });
@@ -802,9 +890,8 @@ int lcb_measure_fma_peak(lcb_ctx* C, int which, double* tflops) {
 //
 // The arena is file-scope device memory: every device on which this
 // library's device code is loaded holds it until the process exits.  In host
-// code its name is only a host-side shadow; the device address is looked up
-// once per device (cudaGetSymbolAddress, with that device current) by the
-// first call on that device.
+// code its name is only a host-side shadow; each call looks up the device
+// address (cudaGetSymbolAddress, with the context's device current).
 //
 // Every call on a device shares the arena, which keeps the previous call's
 // contents.  The accumulators that must start at zero (per-model sums, status
@@ -820,19 +907,18 @@ namespace {
 
 constexpr int kNoallocMaxDevices = 64;
 std::mutex g_noalloc_mu[kNoallocMaxDevices];   // one per device
-void* g_noalloc_base[kNoallocMaxDevices] = {};  // device address of the arena, per device
 
-// The arena's device address on the current device (set up on first use).
-// Caller holds g_noalloc_mu[device] and has made `device` current.
-unsigned char* noalloc_arena(int device) {
-    if (!g_noalloc_base[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
-        if (e != cudaSuccess || !p)
-            throw Error(LCB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc arena): ") + cudaGetErrorString(e));
-        g_noalloc_base[device] = p;
-    }
-    return static_cast<unsigned char*>(g_noalloc_base[device]);
+// The arena's device address on the current device.  Looked up on every call
+// (it is cheap next to the launch sequence), so a device or primary-context
+// reset between calls, which reloads the module at a new address, cannot leave
+// a stale pointer behind.  Caller holds g_noalloc_mu[device] and has made
+// `device` current.
+unsigned char* noalloc_arena() {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
+    if (e != cudaSuccess || !p)
+        throw Error(LCB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc arena): ") + cudaGetErrorString(e));
+    return static_cast<unsigned char*>(p);
 }
 
 // Lays out every buffer of a planned single-model evaluation inside the arena
@@ -923,7 +1009,7 @@ extern "C" int lcb_light_curve_noalloc(lcb_ctx* C, const lcb_model* model, const
                                              std::to_string((size_t)LCB_NOALLOC_ARENA_BYTES) +
                                              "; use lcb_light_curve (or coarser grids / fewer points)");
         std::lock_guard<std::mutex> lock(g_noalloc_mu[C->device]);
-        noalloc_carve(P, noalloc_arena(C->device), D);
+        noalloc_carve(P, noalloc_arena(), D);
         std::vector<double> res, calc;
         std::vector<int> status;
         try {

@@ -166,6 +166,10 @@ constexpr int kElemThreads = 256;
 #endif
 constexpr int kRocheBlock = LCB_ROCHE_BLOCK;       // elements per k_roche block
 
+// Potential evaluations allowed in one line-of-sight search of the eclipse search
+// (the reference has no such bound; a model that reaches it fails: kStatusIterCap).
+constexpr int kFblinkEvalCap = 1 << 18;
+
 // Device status bits (ModelDev.status / batch status word).
 constexpr int kStatusIterCap = 1;     // an iteration cap without a reference counterpart tripped
 constexpr int kStatusTmaTimeout = 2;  // a bounded mbarrier wait gave up

@@ -15,7 +15,8 @@
 //                phase scan with exact lower-bound miss proofs, then the two
 //                bisections.  Small batches run k_roche_scan (the scan split
 //                over several threads, first hit by atomicMin) and
-//                k_roche_chop (the bisections from that hit) instead.
+//                k_roche_chop2 (the ingress and egress bisections from that
+//                hit, one thread each) instead.
 //   k_aux      : per star element, the per-model FP64 sums of ginterp,
 //                wdwarf, log g and radii (flux.rs:115-206, 288-373).
 //   k_flux     : persistent FP32 flux sum (flux.rs:7-111) over work units of
@@ -49,7 +50,6 @@ constexpr double kFac1 = 2.0e27 * 6.6262e-34 * 2.99792458e8;      // planck.rs:5
 constexpr double kFac2 = 1.0e9 * 6.6262e-34 * 2.99792458e8 / 1.3806e-23;  // planck.rs:8
 constexpr double kFwhmEfac = 2.3548200450309493;                  // brightness.rs:8
 constexpr double kEfac = 1.0000001;                               // grid.rs:396
-constexpr int kFblinkEvalCap = 1 << 18;  // bound on one line-of-sight search (reference has none)
 #ifndef LCB_ROCHE_MIN_BLOCKS
 #define LCB_ROCHE_MIN_BLOCKS 5
 #endif
@@ -117,9 +117,12 @@ __device__ __forceinline__ double los_dpot(const RocheEcl& s, const Los& L, doub
     return gx * L.ex + gy * L.ey + gz * L.ez;
 }
 
-// Work counters of the eclipse search (potential and gradient evaluations, fblink calls).
+// Work counters of the eclipse search (potential and gradient evaluations, fblink calls),
+// and the bound on one line-of-sight search's potential evaluations (the reference has
+// none; reaching it marks the model failed: kStatusIterCap).
 struct EclCount {
     int pot = 0, dpot = 0, fbl = 0, cert = 0, skipped = 0;
+    int cap = kFblinkEvalCap;
 };
 
 // dbrent with stop-fast (crates/subs/src/numerical/dbrent.rs:20-165).
@@ -296,7 +299,7 @@ __device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L,
                 if (flam < f1 && flam < f2) { lam = lam + (double)n * step; br = true; break; }
             }
             if (br) break;
-            if (local > kFblinkEvalCap) { capped = true; cnt.pot += local; return false; }
+            if (local > cnt.cap) { capped = true; cnt.pot += local; return false; }
             step /= 2.0;
             nstep *= 2;
         }
@@ -368,8 +371,12 @@ constexpr int kNoHit = 0x7f7f7f7f;  // first-hit sentinel (the byte pattern a me
 
 // `known_hit` >= 0: the scan's first hit is already known (split scan): go
 // straight to the bisections from that phase; kNoHit: the point is not eclipsed.
+// `only` = 1 or 2 runs just the ingress or just the egress bisection (the two are
+// independent: both start from the first hit), leaving `ing` resp. the unwrapped
+// `eg` set; the caller then applies egress < ingress -> egress + 1 itself.
 __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
-                               double pz, double& ing, double& eg, bool& capped, EclCount& evals, int known_hit = -1) {
+                               double pz, double& ing, double& eg, bool& capped, EclCount& evals, int known_hit = -1,
+                               int only = 0) {
     Scan sc;
     if (!scan_setup(s, cosi, sini, delta, px, py, pz, sc)) return false;
     if (known_hit == kNoHit) return false;
@@ -381,7 +388,8 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
     double phi = 0.0, pin = 0.0, pout = 0.0;
     if (known_hit >= 0) {  // as the scan below sets up its first hit
         phi = phi1 + (double)known_hit * dphi;
-        mode = CHOP_IN; pin = phi; pout = phi1;
+        if (only == 2) { mode = CHOP_EG; pin = phi; pout = phi2; }
+        else { mode = CHOP_IN; pin = phi; pout = phi1; }
     }
     for (;;) {
         double ph;
@@ -394,10 +402,12 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
                 r -= floor(r);
                 if (mode == CHOP_IN) {
                     ing = r;
+                    if (only == 1) return true;
                     mode = CHOP_EG; pin = phi; pout = phi2; it = 0;
                     continue;
                 }
                 eg = r;
+                if (only == 2) return true;
                 if (eg < ing) eg += 1.0;
                 return true;
             }
@@ -778,6 +788,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs
     const SegDesc sg = A.segs[blk.seg];
     const int64_t i = blk.offset + threadIdx.x;
     EclCount cnt;
+    cnt.cap = A.fblink_cap;
     bool capped = false;
     if (i < sg.count) {
         const ModelDev& M = A.models[sg.model];
@@ -836,6 +847,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(Ele
     const SegDesc sg = A.segs[blk.seg];
     const int64_t i = blk.offset + threadIdx.x;
     EclCount cnt;
+    cnt.cap = A.fblink_cap;
     bool capped = false;
     if (i < sg.count) {
         const ModelDev& M = A.models[sg.model];
@@ -848,26 +860,41 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(Ele
     roche_counters(A, cnt);
 }
 
-// Split scan, second kernel: the bisections from the first hit.
-__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop(ElemArgs A) {
-    const ElemBlock blk = A.rblocks[blockIdx.x];
+// Split scan, second kernel with two threads per element: adjacent lanes run
+// the ingress and the egress bisection of one element at once (each from the
+// first hit, eclipse.rs:301-332), halving the longest chain of line-of-sight
+// searches; the ingress lane combines the pair.  Block b covers half of Roche
+// block b / 2.
+__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(ElemArgs A) {
+    const int64_t rb = blockIdx.x >> 1;
+    const int slot = (int)(blockIdx.x & 1) * (kRocheBlock / 2) + (int)(threadIdx.x >> 1);
+    const int part = threadIdx.x & 1;  // 0: ingress, 1: egress
+    const ElemBlock blk = A.rblocks[rb];
     const SegDesc sg = A.segs[blk.seg];
-    const int64_t i = blk.offset + threadIdx.x;
+    const int64_t i = blk.offset + slot;
     EclCount cnt;
-    bool capped = false;
+    cnt.cap = A.fblink_cap;
+    bool capped = false, found = false;
+    double a = 0.0, b = 0.0;
+    int64_t e = 0;
     if (i < sg.count) {
         const ModelDev& M = A.models[sg.model];
         const RocheEcl& R = blk.by == 1 ? M.ecl1 : M.ecl2;
-        const int64_t e = sg.first + i;
+        e = sg.first + i;
         const double4 p = A.el_p64[e];
-        const int first = A.firsthit[(int64_t)blockIdx.x * kRocheBlock + threadIdx.x];
+        const int first = A.firsthit[rb * kRocheBlock + slot];
         Scan sc;
-        if (scan_setup(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, sc))
+        if (part == 0 && scan_setup(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, sc))
             cnt.fbl += first == kNoHit ? sc.nsteps + 1 : first + 1;  // the single scan's searches
-        double a, b;
-        if (ingress_egress(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt, first))
-            A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, blk.by)] = make_double2(a, b);
-        if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
+        found = ingress_egress(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt, first, part + 1);
+    }
+    const double egress = __shfl_xor_sync(0xffffffffu, b, 1);
+    const bool found_eg = __shfl_xor_sync(0xffffffffu, (int)found, 1) != 0;
+    const bool capped_eg = __shfl_xor_sync(0xffffffffu, (int)capped, 1) != 0;
+    if (i < sg.count && part == 0) {
+        if (found && found_eg) A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, blk.by)] =
+            make_double2(a, egress < a ? egress + 1.0 : egress);
+        if (capped || capped_eg) atomicOr(A.status + sg.model, kStatusIterCap);
     }
     roche_counters(A, cnt);
 }
@@ -1019,15 +1046,35 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait (about 2 s of SM clock); on time-out the caller records an error.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: gives up after `limit` SM clock cycles (by default about 2 s);
+// on time-out the caller records an error status instead of hanging.
+constexpr long long kWaitLimit = 4000000000LL;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kWaitLimit) {
     if (mbar_test(bar, parity)) return true;
     long long t0 = clock64();
     while (!mbar_test(bar, parity)) {
         __nanosleep(64);
-        if (clock64() - t0 > 4000000000LL) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
+}
+
+// The bounded wait on an mbarrier that nothing completes (no copy, no arrival):
+// it must give up after `limit` cycles and report kStatusTmaTimeout.
+__global__ void k_wait_probe(long long limit, int* status, long long* waited) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const long long t0 = clock64();
+    const bool ok = mbar_wait(&bar, 0u, limit);
+    const long long t1 = clock64();
+    if (threadIdx.x == 0) {
+        *status = ok ? 0 : kStatusTmaTimeout;
+        *waited = t1 - t0;
+    }
 }
 
 enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
@@ -1769,6 +1816,11 @@ cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflo
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+cudaError_t launch_wait_probe(long long limit, int* status, long long* waited, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(limit, status, waited);
+    return cudaGetLastError();
+}
+
 size_t flux_smem_bytes() { return flux_smem_bytes_impl(); }
 
 // The flux kernel's dynamic shared memory exceeds the 48 KB default; the
@@ -1813,7 +1865,7 @@ cudaError_t launch_roche(const ElemArgs& a, cudaStream_t s) {
     k_roche_scan<<<(unsigned)(a.nrblocks * a.roche_split), kRocheBlock, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_roche_chop<<<(unsigned)a.nrblocks, kRocheBlock, 0, s>>>(a);
+    k_roche_chop2<<<(unsigned)(2 * a.nrblocks), kRocheBlock, 0, s>>>(a);
     return cudaGetLastError();
 }
 

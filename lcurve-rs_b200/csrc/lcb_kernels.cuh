@@ -27,6 +27,7 @@ struct ElemArgs {
     unsigned long long* counters;  // [pot evals, dpot evals, fblink calls, bound nodes, proven misses] or null
     int roche_split;     // threads per Roche-eclipsed element in the phase scan (1: one kernel)
     int* firsthit;       // split scan: first hit per Roche thread (nrblocks x kRocheBlock), starts at 0x7f7f7f7f
+    int fblink_cap;      // potential evaluations allowed in one line-of-sight search (kFblinkEvalCap)
 };
 
 struct PhaseArgs {
@@ -85,5 +86,7 @@ cudaError_t launch_flux(const FluxArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_epilogue(const EpiArgs& a, cudaStream_t s);
 int flux_blocks_per_sm();
 cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflops);
+// One block waiting on an mbarrier that nothing completes, bounded by `limit` cycles.
+cudaError_t launch_wait_probe(long long limit, int* status, long long* waited, cudaStream_t s);
 
 }  // namespace lcb

@@ -87,3 +87,96 @@ def light_curve_sharded(model, data: np.ndarray, scale: bool = False, group=None
     for k in range(5):
         res.sfac[k] = s
     return LcResult(data["time"], calc, res)
+
+
+# ---------------------------------------------------------------------------
+# One batch of models split across GPUs by cost (the reference's chisq_batch
+# model loop, orchestration.rs:343-356, distributed over ranks)
+# ---------------------------------------------------------------------------
+# Device time per unit of work on a B200, measured on the 1024-model batch
+# (k_flux, k_roche and k_elements stage times over their work counts), in
+# units of one flux element-evaluation: an element eclipsed by a Roche-
+# distorted star costs about 17,500 of them in the eclipse search, any grid
+# element about 330 in the grid/continuum kernel.
+ROCHE_WEIGHT = 17_500
+ELEMENT_WEIGHT = 330
+
+
+def model_costs(models, data: np.ndarray, offsets) -> np.ndarray:
+    """Work estimate of each model of a ragged batch on its own data: flux
+    element-evaluations + ROCHE_WEIGHT x Roche-eclipsed elements +
+    ELEMENT_WEIGHT x grid elements (lcb_model_work: host planning only, no
+    device work).  Physically invalid models cost 0."""
+    from . import _capi  # noqa: PLC0415
+    L = _capi.load()
+    data = np.ascontiguousarray(data, dtype=DATUM_DTYPE)
+    offs = np.asarray(offsets, dtype=np.int64)
+    out = np.zeros(len(models))
+    w = np.zeros(4, dtype=np.int64)
+    for i, m in enumerate(models):
+        lo, hi = int(offs[i]), int(offs[i + 1])
+        _capi.check(L.lcb_model_work(m._h, data[lo:].ctypes.data, hi - lo, _capi.i64ptr(w)))
+        out[i] = float(w[3]) + ROCHE_WEIGHT * float(w[1]) + ELEMENT_WEIGHT * float(w[0])
+    return out
+
+
+def partition(costs, world: int) -> list[np.ndarray]:
+    """Models per rank: longest processing time first, each model to the rank
+    with the least work so far (ties to the lower rank); every rank computes
+    the same split.  Each rank's indices are returned in ascending order."""
+    costs = np.asarray(costs, dtype=np.float64)
+    order = sorted(range(costs.size), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    owner = np.zeros(costs.size, dtype=np.int64)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += costs[i]
+    return [np.flatnonzero(owner == r) for r in range(world)]
+
+
+def _evaluate_batch_engine(models, data, offsets, scale):
+    from . import chisq_batch_ragged  # noqa: PLC0415
+    return chisq_batch_ragged(models, data, offsets, scale=scale)[0]
+
+
+def chisq_batch_sharded(models, data: np.ndarray, offsets, scale: bool = False, group=None, evaluate=None,
+                        costs=None) -> np.ndarray:
+    """Chi-squared of every model of a ragged batch (model i on data[offsets[i]
+    : offsets[i+1]]), the models divided among the ranks of `group` by cost
+    (model_costs, partition); each rank evaluates its models in one batch and
+    the per-model results are all-gathered, so every rank returns the whole
+    batch's chi-squared (NaN for failed models, as chisq_batch_ragged).
+    Every rank passes the same models, data and offsets.
+
+    evaluate(models, data, offsets, scale) -> chisq evaluates one rank's
+    share; by default the GPU engine (chisq_batch_ragged)."""
+    data = np.ascontiguousarray(data, dtype=DATUM_DTYPE)
+    offs = np.asarray(offsets, dtype=np.int64)
+    n = len(models)
+    evaluate = evaluate or _evaluate_batch_engine
+    if group is None:
+        return np.asarray(evaluate(list(models), data, offs, scale), dtype=np.float64)
+    import torch  # noqa: PLC0415
+    import torch.distributed as dist  # noqa: PLC0415
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    if costs is None:
+        costs = model_costs(models, data, offs)
+    parts = partition(costs, world)
+    mine = parts[rank]
+    local = np.zeros(0)
+    if mine.size:
+        sub = np.concatenate([data[offs[i]:offs[i + 1]] for i in mine])
+        soffs = np.zeros(mine.size + 1, dtype=np.int64)
+        soffs[1:] = np.cumsum([offs[i + 1] - offs[i] for i in mine])
+        local = np.asarray(evaluate([models[i] for i in mine], sub, soffs, scale), dtype=np.float64)
+    width = max(max(p.size for p in parts), 1)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+    buf = torch.zeros(width, dtype=torch.float64, device=dev)
+    buf[:local.size] = torch.as_tensor(local, dtype=torch.float64)
+    got = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(got, buf, group=group)
+    out = np.empty(n)
+    for r in range(world):
+        out[parts[r]] = got[r][:parts[r].size].cpu().numpy()
+    return out

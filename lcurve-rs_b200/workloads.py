@@ -175,6 +175,25 @@ def batch_models(n=1024, seed=1234, nlat1=(30, 300), nlat2=(30, 500), ntime=(200
     return out
 
 
+def workload_key(specs) -> str:
+    """SHA-1 of a batch's model texts and time grids (identifies a batch_models draw)."""
+    import hashlib  # noqa: PLC0415
+    h = hashlib.sha1()
+    for text, t in specs:
+        h.update(text.encode())
+        h.update(np.ascontiguousarray(t, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def batch_noise(fid_flux, seed):
+    """The batch's observed fluxes and errors: the fiducial (single_small) curve
+    at every model's times plus N(0, (0.01 flux)^2), from default_rng(seed + 99)."""
+    rng = np.random.default_rng(seed + 99)
+    fid_flux = np.asarray(fid_flux, dtype=np.float64)
+    sig = 0.01 * np.abs(fid_flux)
+    return fid_flux + sig * rng.standard_normal(fid_flux.shape), sig
+
+
 def noisy_data(times, flux, expose, ndiv, seed, frac=0.01):
     """Data records: flux + N(0, (frac*flux)^2), ferr = frac*flux, weight 1."""
     from . import make_data  # noqa: PLC0415
@@ -184,3 +203,72 @@ def noisy_data(times, flux, expose, ndiv, seed, frac=0.01):
     d = make_data(times, expose=expose, ndiv=ndiv, flux=flux + sig * rng.standard_normal(flux.shape), ferr=sig,
                   weight=1.0)
     return d
+
+
+def roche_lobe_eggleton(q_donor: float) -> float:
+    """Eggleton (1983) volume-equivalent Roche-lobe radius, in units of the
+    separation, of a star of mass ratio q_donor = M_star / M_companion."""
+    a, b = q_donor ** (2.0 / 3.0), q_donor ** (1.0 / 3.0)
+    return 0.49 * a / (0.6 * a + np.log(1.0 + b))
+
+
+SWEEP_KINDS = ("roche_secondary", "sphere_secondary", "eclipse_flags", "gravity_darkening", "limb_laws",
+               "disc", "bright_spot", "disc_spot_gd", "edge")
+
+
+def model_sweep(n=100, seed=42):
+    """Seeded models across the path's physical options, for parity sweeps at
+    small grids (the base model's nlat 20/40, disc nrad 40): Roche-filling and
+    spherical secondaries, eclipse flags on and off, gravity darkening with
+    bolometric or band exponents, polynomial and Claret limb darkening, discs
+    (opaque or not), bright spots, and edge cases (low inclination, q = 1,
+    negative t2, mirror irradiation, a Roche-distorted primary).  Returns
+    [(kind, text)]."""
+    rng = np.random.default_rng(seed)
+    u = lambda lo, hi: float(rng.uniform(lo, hi))  # noqa: E731
+    out = []
+    for i in range(n):
+        kind = SWEEP_KINDS[i * len(SWEEP_KINDS) // n]
+        o = dict(q=u(0.1, 0.9), iangle=u(66.0, 88.0), r1=u(0.008, 0.035), t1=u(9000.0, 28000.0),
+                 t2=u(2800.0, 5500.0))
+        if kind == "roche_secondary":
+            o["absorb"] = u(0.0, 1.0)
+        elif kind == "sphere_secondary":
+            o.update(roche2=0, r2=u(0.1, min(0.4, 0.9 * roche_lobe_eggleton(o["q"]))))
+        elif kind == "eclipse_flags":
+            o.update(eclipse1=i % 2, eclipse2=(i // 2) % 2)
+        elif kind == "gravity_darkening":
+            o.update(gravity_dark1=u(0.08, 0.32), gravity_dark2=u(0.08, 0.32), absorb=u(0.0, 1.0),
+                     gdark_bolom1=int(rng.integers(0, 2)), gdark_bolom2=int(rng.integers(0, 2)))
+        elif kind == "limb_laws":
+            for s in ("1", "2"):
+                o[f"limb{s}"] = "Claret" if rng.integers(0, 2) else "Poly"
+                for k, (lo, hi) in enumerate(((0.1, 0.8), (-0.5, 0.5), (-0.3, 0.3), (-0.2, 0.2)), start=1):
+                    o[f"ldc{s}_{k}"] = u(lo, hi)
+        if kind in ("disc", "bright_spot", "disc_spot_gd"):
+            rl1 = roche_lobe_eggleton(1.0 / o["q"])
+            rdisc2 = u(0.2, min(0.45, 0.9 * rl1))
+            o.update(add_disc=1, opaque=int(rng.integers(0, 2)), rdisc1=o["r1"] + u(0.01, 0.03), rdisc2=rdisc2,
+                     height_disc=u(0.02, 0.15), beta_disc=u(1.0, 2.0), temp_disc=u(2000.0, 8000.0),
+                     texp_disc=u(-2.5, -0.5), lin_limb_disc=u(0.1, 0.6), quad_limb_disc=u(-0.2, 0.3))
+        if kind in ("bright_spot", "disc_spot_gd"):
+            o.update(add_spot=1, radius_spot=o["rdisc2"] * u(0.8, 1.0), length_spot=u(0.01, 0.05),
+                     height_spot=u(0.02, 0.1), expon_spot=u(0.0, 2.0), epow_spot=u(0.5, 2.0),
+                     angle_spot=u(100.0, 180.0), yaw_spot=u(-20.0, 20.0), temp_spot=u(8000.0, 25000.0),
+                     tilt_spot=u(60.0, 120.0), cfrac_spot=u(0.05, 0.5))
+        if kind == "disc_spot_gd":
+            o.update(gravity_dark1=u(0.08, 0.32), gravity_dark2=u(0.08, 0.32))
+        if kind == "edge":
+            case = i % 5
+            if case == 0:
+                o.update(iangle=30.0)                     # no eclipses
+            elif case == 1:
+                o.update(q=1.0, iangle=80.0, r1=0.01)     # equal masses
+            elif case == 2:
+                o.update(t2=-0.3, iangle=78.0)            # t2 < 0: the secondary's temperature by irradiation
+            elif case == 3:
+                o.update(q=0.4, iangle=82.0, mirror=1)    # mirror irradiation term
+            else:
+                o.update(q=0.6, iangle=80.0, r1=0.02, roche1=1)  # Roche-distorted primary
+        out.append((kind, model_text(**o)))
+    return out

@@ -18,10 +18,10 @@
 // the reference's own bound (tests/regression.rs:84-88).
 //
 // Parallelism mirrors the reference's Rayon loops: over times inside one
-// light curve (crates/lcurve/src/orchestration.rs:229) and over models in
-// chisq_batch (orchestration.rs:343).  Nested parallel regions run serially
-// inside a worker, which gives the same work distribution when there are
-// more models than threads.
+// light curve (crates/lcurve/src/orchestration.rs:229), over models in
+// chisq_batch (orchestration.rs:343) and over elements in the continuum
+// (brightness.rs:50,119).  The loops nest as Rayon's do: threads that run out
+// of models help with the time loops of the models still running.
 
 #include <algorithm>
 #include <atomic>
@@ -32,8 +32,10 @@
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <condition_variable>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -1234,6 +1236,23 @@ struct GridArgs {
     Star which;
 };
 
+// An element's eclipse intervals are a function of its position alone.  The
+// builders below compute them element by element, as the reference does
+// (grid.rs:227-320: serial per star), unless orc_set_grid_threads(n > 1) was
+// called: then each builder computes them after its loop, n threads over its
+// elements -- the same function of the same inputs, so the same grid, built
+// faster.  Only the full-size parity tests use that.
+static int g_grid_threads = 1;
+template <class F>
+static void parallel_for(int64_t n, int nthreads, F&& f);
+template <class F>
+static void grid_eclipses(std::vector<Point>& pts, size_t first, F&& ecl_of) {
+    parallel_for((int64_t)(pts.size() - first), g_grid_threads, [&](int64_t i) {
+        Point& p = pts[first + (size_t)i];
+        ecl_of(p.posn, p.eclipse);
+    });
+}
+
 // grid.rs:201-322
 static void add_faces(std::vector<Point>& star, double tlo, double thi, double dtheta, int nlatfill, int nlngfill,
                       const Model& mdl, const GridArgs& g) {
@@ -1248,6 +1267,17 @@ static void add_faces(std::vector<Point>& star, double tlo, double thi, double d
         nlat = sat_i32(std::ceil((thi - tlo) / dtheta));
     }
     const double q = mdl.v(Q);
+    const size_t first = star.size();
+    const bool defer = g_grid_threads > 1;
+    auto ecl_of = [&](const Vec3& posn, EclipseVec& eclipses) {
+        if (!g.eclipse) return;
+        if (g.which == PRIMARY)
+            star_eclipse(q, g.r2, mdl.v(SPIN2), g.ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2,
+                         SECONDARY, eclipses);
+        else
+            star_eclipse(q, g.r1, mdl.v(SPIN1), g.ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1,
+                         PRIMARY, eclipses);
+    };
     for (int64_t nt = 0; nt < nlat; ++nt) {
         double theta, phi1, phi2;
         int64_t nphi, nl;
@@ -1294,17 +1324,11 @@ static void add_faces(std::vector<Point>& star, double tlo, double thi, double d
             double area = ((phi2 - phi1) / (double)nphi * rad * sint) * ((thi - tlo) / (double)nl * rad) /
                           Vec3::dot(dirn, dvec);
             EclipseVec eclipses;
-            if (g.eclipse) {
-                if (g.which == PRIMARY)
-                    star_eclipse(q, g.r2, mdl.v(SPIN2), g.ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2,
-                                 SECONDARY, eclipses);
-                else
-                    star_eclipse(q, g.r1, mdl.v(SPIN1), g.ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1,
-                                 PRIMARY, eclipses);
-            }
+            if (!defer) ecl_of(posn, eclipses);
             star.push_back(make_point(posn, dvec, area, gravity / g.gref, eclipses));
         }
     }
+    if (defer) grid_eclipses(star, first, ecl_of);
 }
 
 static std::vector<Point> set_star_grid_inner(const Model& mdl, Star which, GridArgs g, int nlat, bool infill,
@@ -1403,6 +1427,12 @@ std::vector<Point> set_disc_grid(const Model& mdl) {
     double drad = (rdisc2 - rdisc1) / (double)mdl.nrad;
     double drrad = rdisc2 / (double)mdl.nrad;
     std::vector<Point> disc;
+    const bool defer = g_grid_threads > 1;
+    auto ecl_of = [&](const Vec3& posn, EclipseVec& ecl) {
+        if (mdl.opaque) ecl = disc_eclipse(mdl.v(IANGLE), rdisc1, rdisc2, mdl.v(BETA_DISC), mdl.v(HEIGHT_DISC), posn);
+        if (mdl.eclipse1) star_eclipse(q, r1, mdl.v(SPIN1), ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1, PRIMARY, ecl);
+        if (mdl.eclipse2) star_eclipse(q, r2, mdl.v(SPIN2), ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2, SECONDARY, ecl);
+    };
     for (int i = 0; i < mdl.nrad; ++i) {
         double rad = rdisc1 + (rdisc2 - rdisc1) * ((double)i + 0.5) / (double)mdl.nrad;
         int64_t ntheta = std::max<int64_t>(8, sat_i32(std::ceil(TWOPI * rad / drrad)));
@@ -1417,12 +1447,11 @@ std::vector<Point> set_disc_grid(const Model& mdl) {
             Vec3 posn(rad * cost, rad * sint, h);
             Vec3 dirn(-cost * sinp, -sint * sinp, cosp);
             EclipseVec ecl;
-            if (mdl.opaque) ecl = disc_eclipse(mdl.v(IANGLE), rdisc1, rdisc2, mdl.v(BETA_DISC), mdl.v(HEIGHT_DISC), posn);
-            if (mdl.eclipse1) star_eclipse(q, r1, mdl.v(SPIN1), ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1, PRIMARY, ecl);
-            if (mdl.eclipse2) star_eclipse(q, r2, mdl.v(SPIN2), ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2, SECONDARY, ecl);
+            if (!defer) ecl_of(posn, ecl);
             disc.push_back(make_point(posn, dirn, area, 1.0, ecl));
         }
     }
+    if (defer) grid_eclipses(disc, 0, ecl_of);
     return disc;
 }
 
@@ -1446,14 +1475,18 @@ std::vector<Point> set_disc_edge(const Model& mdl, bool outer) {
     int64_t ntheta = std::max<int64_t>(8, sat_i32(std::ceil(TWOPI * rad_val / size)));
     double area = TWOPI / (double)ntheta * rad_val * 2.0 * h / (double)(nout - 1);
     std::vector<Point> edge;
-    auto eclipses_for = [&](const Vec3& posn) {
-        EclipseVec ecl;
+    const bool defer = g_grid_threads > 1;
+    auto ecl_of = [&](const Vec3& posn, EclipseVec& ecl) {
         if (mdl.opaque) ecl = disc_eclipse(mdl.v(IANGLE), rdisc1, rdisc2, mdl.v(BETA_DISC), mdl.v(HEIGHT_DISC), posn);
         if (mdl.eclipse1) {
             try { star_eclipse(q, r1, mdl.v(SPIN1), ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1, PRIMARY, ecl); }
             catch (const RocheError&) {}
         }
         if (mdl.eclipse2) star_eclipse(q, r2, mdl.v(SPIN2), ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2, SECONDARY, ecl);
+    };
+    auto eclipses_for = [&](const Vec3& posn) {
+        EclipseVec ecl;
+        if (!defer) ecl_of(posn, ecl);
         return ecl;
     };
     for (int64_t i = 0; i < ntheta; ++i) {
@@ -1471,6 +1504,7 @@ std::vector<Point> set_disc_edge(const Model& mdl, bool outer) {
             edge.push_back(make_point(p2, d2, area, 1.0, eclipses_for(p2)));
         }
     }
+    if (defer) grid_eclipses(edge, 0, ecl_of);
     return edge;
 }
 
@@ -1501,12 +1535,16 @@ std::vector<Point> set_bright_spot_grid(const Model& mdl, Vec3* bspot_out = null
     double area = sfac * mdl.v(LENGTH_SPOT) * mdl.v(HEIGHT_SPOT) / (double)(mdl.nspot - 1);
     double bright_ref = planck(mdl.wavelength, mdl.v(TEMP_SPOT));
     std::vector<Point> spot;
+    const bool defer = g_grid_threads > 1;
+    auto ecl_of = [&](const Vec3& posn, EclipseVec& ecl) {
+        if (mdl.eclipse1) star_eclipse(q, r1, mdl.v(SPIN1), ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1, PRIMARY, ecl);
+        if (mdl.eclipse2) star_eclipse(q, r2, mdl.v(SPIN2), ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2, SECONDARY, ecl);
+    };
     for (int i = 0; i < mdl.nspot; ++i) {
         double dist = sfac * (double)i / (double)(mdl.nspot - 1);
         Vec3 posn = bspot + (mdl.v(LENGTH_SPOT) * (dist - bmax)) * bvec;
         EclipseVec ecl;
-        if (mdl.eclipse1) star_eclipse(q, r1, mdl.v(SPIN1), ffac1, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche1, PRIMARY, ecl);
-        if (mdl.eclipse2) star_eclipse(q, r2, mdl.v(SPIN2), ffac2, mdl.v(IANGLE), posn, mdl.delta_phase, mdl.roche2, SECONDARY, ecl);
+        if (!defer) ecl_of(posn, ecl);
         double bright = bright_ref * std::pow(dist / bmax, mdl.v(EXPON_SPOT)) *
                         std::exp(mdl.v(EXPON_SPOT) / mdl.v(EPOW_SPOT) - std::pow(dist, mdl.v(EPOW_SPOT)));
         Point pt = make_point(posn, tvec, area, 1.0, ecl);
@@ -1516,6 +1554,7 @@ std::vector<Point> set_bright_spot_grid(const Model& mdl, Vec3* bspot_out = null
         pp.flux = (float)(bright * mdl.v(CFRAC_SPOT) * area);
         spot.push_back(pp);
     }
+    if (defer) grid_eclipses(spot, 0, ecl_of);
     return spot;
 }
 
@@ -1906,35 +1945,119 @@ static double comp_radius(const Pts& star, const Vec3& cofm) {
 }
 
 // ---------------------------------------------------------------------------
-// thread pool (stands in for Rayon's into_par_iter)
+// thread pool (stands in for Rayon's work-stealing into_par_iter)
+//
+// A parallel loop publishes its index range as a job.  Idle workers take
+// chunks of indices from the newest open job, and a thread that waits for its
+// own loop to finish helps jobs opened after its own (loops nested inside
+// other threads' iterations) instead of sleeping.  Loops therefore nest as
+// Rayon's do: in chisq_batch (orchestration.rs:343) threads that run out of
+// models help with the time loops (orchestration.rs:229) of the models still
+// running.  One pool of nthreads - 1 workers exists per thread count.
 // ---------------------------------------------------------------------------
-static thread_local bool t_in_worker = false;
+class Pool {
+    struct Job {
+        const std::function<void(int64_t)>* fn = nullptr;
+        int64_t n = 0, chunk = 1;
+        std::atomic<int64_t> next{0}, done{0};
+        int users = 0;  // threads inside work() on this job (guarded by the pool mutex)
+        uint64_t seq = 0;
+        std::exception_ptr err;
+    };
+    std::mutex mu_;
+    std::condition_variable cv_;  // new job, job finished, job released
+    std::vector<Job*> open_;
+    uint64_t seq_ = 0;
+    std::vector<std::thread> workers_;
+
+    // Newest open job with unclaimed indices (and, for a waiting caller, newer than `after`).
+    Job* pick(uint64_t after) {
+        for (size_t k = open_.size(); k-- > 0;) {
+            Job* j = open_[k];
+            if (j->seq > after && j->next.load() < j->n) { ++j->users; return j; }
+        }
+        return nullptr;
+    }
+    void work(Job* j) {
+        for (;;) {
+            int64_t i0 = j->next.fetch_add(j->chunk);
+            if (i0 >= j->n) break;
+            int64_t i1 = std::min(j->n, i0 + j->chunk);
+            for (int64_t i = i0; i < i1; ++i) {
+                try { (*j->fn)(i); }
+                catch (...) {
+                    std::lock_guard<std::mutex> g(mu_);
+                    if (!j->err) j->err = std::current_exception();
+                }
+            }
+            flush_counters();
+            if (j->done.fetch_add(i1 - i0) + (i1 - i0) == j->n) {
+                std::lock_guard<std::mutex> g(mu_);
+                cv_.notify_all();
+            }
+        }
+        std::lock_guard<std::mutex> g(mu_);
+        if (--j->users == 0) cv_.notify_all();
+    }
+
+public:
+    explicit Pool(int nthreads) {
+        for (int t = 1; t < nthreads; ++t)
+            workers_.emplace_back([this] {
+                for (;;) {
+                    Job* j = nullptr;
+                    {
+                        std::unique_lock<std::mutex> lk(mu_);
+                        cv_.wait(lk, [&] { return (j = pick(0)) != nullptr; });
+                    }
+                    work(j);
+                }
+            });
+        for (auto& w : workers_) w.detach();  // process-lifetime pool
+    }
+    static Pool& get(int nthreads) {
+        static std::mutex m;
+        static std::map<int, Pool*> pools;
+        std::lock_guard<std::mutex> g(m);
+        Pool*& p = pools[nthreads];
+        if (!p) p = new Pool(nthreads);
+        return *p;
+    }
+    void run(int64_t n, int nthreads, const std::function<void(int64_t)>& fn) {
+        Job j;
+        j.fn = &fn;
+        j.n = n;
+        j.chunk = std::max<int64_t>(1, n / (64 * (int64_t)nthreads));
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            j.seq = ++seq_;
+            j.users = 1;
+            open_.push_back(&j);
+            cv_.notify_all();
+        }
+        work(&j);
+        std::unique_lock<std::mutex> lk(mu_);
+        while (j.done.load() < n) {
+            Job* other = pick(j.seq);
+            if (!other) { cv_.wait(lk); continue; }
+            lk.unlock();
+            work(other);
+            lk.lock();
+        }
+        open_.erase(std::find(open_.begin(), open_.end(), &j));
+        cv_.wait(lk, [&] { return j.users == 0; });
+        if (j.err) std::rethrow_exception(j.err);
+    }
+};
+
 template <class F>
 static void parallel_for(int64_t n, int nthreads, F&& f) {
-    if (nthreads <= 1 || t_in_worker || n < 2) {
+    if (nthreads <= 1 || n < 2) {
         for (int64_t i = 0; i < n; ++i) f(i);
         return;
     }
-    std::atomic<int64_t> next{0};
-    int nt = (int)std::min<int64_t>(nthreads, n);
-    std::vector<std::thread> th;
-    std::vector<std::exception_ptr> errs(nt);
-    for (int t = 0; t < nt; ++t) {
-        th.emplace_back([&, t] {
-            t_in_worker = true;
-            try {
-                for (;;) {
-                    int64_t i = next.fetch_add(1);
-                    if (i >= n) break;
-                    f(i);
-                }
-            } catch (...) { errs[t] = std::current_exception(); }
-            flush_counters();
-            t_in_worker = false;
-        });
-    }
-    for (auto& x : th) x.join();
-    for (auto& e : errs) if (e) std::rethrow_exception(e);
+    const std::function<void(int64_t)> fn = [&](int64_t i) { f(i); };
+    Pool::get(nthreads).run(n, nthreads, fn);
 }
 
 // ---------------------------------------------------------------------------
@@ -2126,16 +2249,14 @@ static inline double datum_phase(const Model& mdl, double time) {  // orchestrat
     return phase;
 }
 
-// orchestration.rs:36-318
-LcResult light_curve_comp(const Model& mdl, const std::vector<Datum>& data, bool scale, bool rdata, int nthreads,
-                          Grids* keep = nullptr) {
+// orchestration.rs:171-318: the time loop, scaling and the per-star sums, on grids
+// already built by build_grids.
+LcResult light_curve_on(const Model& mdl, const Grids& G, const std::vector<Datum>& data, bool scale, bool rdata,
+                        int nthreads) {
     if (data.empty()) throw std::runtime_error("light_curve_comp: no data");
     size_t n = data.size();
     LcResult res;
     res.calc.assign(n, 0.0);
-    Grids Gl;
-    Grids& G = keep ? *keep : Gl;
-    build_grids(mdl, G, nthreads);
     double xmin = data[0].time, xmax = data[0].time;
     for (size_t i = 1; i < n; ++i) { if (data[i].time < xmin) xmin = data[i].time; if (data[i].time > xmax) xmax = data[i].time; }
     double middle = (xmin + xmax) / 2.0, range = (xmax - xmin) / 2.0;
@@ -2207,6 +2328,14 @@ LcResult light_curve_comp(const Model& mdl, const std::vector<Datum>& data, bool
     res.rv1 = comp_radius(G.star1f, Vec3());
     res.rv2 = comp_radius(G.star2f, Vec3(1.0, 0.0, 0.0));
     return res;
+}
+
+// orchestration.rs:36-318
+LcResult light_curve_comp(const Model& mdl, const std::vector<Datum>& data, bool scale, bool rdata, int nthreads) {
+    if (data.empty()) throw std::runtime_error("light_curve_comp: no data");
+    Grids G;
+    build_grids(mdl, G, nthreads);
+    return light_curve_on(mdl, G, data, scale, rdata, nthreads);
 }
 
 }  // namespace orc
@@ -2304,7 +2433,7 @@ int orc_chisq_batch(void* base, const Datum* data, int n, const char** names, in
             int k = phys_index(names[j]);
             if (k >= 0) m.p[k].value = values[(size_t)i * ndim + j];
         }
-        try { out[i] = light_curve_comp(m, d, scale != 0, true, 1).chisq; }
+        try { out[i] = light_curve_comp(m, d, scale != 0, true, nthreads).chisq; }
         catch (const std::exception&) { out[i] = NAN; }
     });
     flush_counters();
@@ -2316,24 +2445,43 @@ int orc_chisq_ragged(void** models, int nmodels, const Datum* data, const int64_
                      double* out) {
     parallel_for(nmodels, nthreads, [&](int64_t i) {
         std::vector<Datum> d(data + offsets[i], data + offsets[i + 1]);
-        try { out[i] = light_curve_comp(((OrcModel*)models[i])->m, d, scale != 0, true, 1).chisq; }
+        try { out[i] = light_curve_comp(((OrcModel*)models[i])->m, d, scale != 0, true, nthreads).chisq; }
         catch (const std::exception&) { out[i] = NAN; }
     });
     flush_counters();
     return 0;
 }
 
+// Threads the grid builders use for eclipse intervals (1 = element by element,
+// as the reference); the full-size parity tests raise it.
+void orc_set_grid_threads(int n) { g_grid_threads = n < 1 ? 1 : n; }
+
 // Grid extraction for per-element parity tests.
 int orc_grids_build(void* mh, void** out, char* err, int errlen) {
     try {
         auto* g = new OrcGrids();
-        build_grids(((OrcModel*)mh)->m, g->g, 1);
+        build_grids(((OrcModel*)mh)->m, g->g, g_grid_threads);
         flush_counters();
         *out = g;
         return 0;
     } catch (const std::exception& e) { flush_counters(); set_err(err, errlen, e.what()); return 1; }
 }
 void orc_grids_free(void* g) { delete (OrcGrids*)g; }
+// The light curve of a model on grids already built for it by orc_grids_build
+// (the time loop and everything after it, orchestration.rs:171-318).
+int orc_grids_light_curve(void* gh, void* mh, const Datum* data, int n, int scale, int rdata, int nthreads,
+                          double* calc, double* scalars, char* err, int errlen) {
+    try {
+        std::vector<Datum> d(data, data + n);
+        LcResult r = light_curve_on(((OrcModel*)mh)->m, ((OrcGrids*)gh)->g, d, scale != 0, rdata != 0, nthreads);
+        flush_counters();
+        for (int i = 0; i < n; ++i) calc[i] = r.calc[i];
+        double s[12] = {r.wdwarf, r.chisq, r.wnok, r.logg1, r.logg2, r.rv1, r.rv2,
+                        r.sfac[0], r.sfac[1], r.sfac[2], r.sfac[3], r.sfac[4]};
+        if (scalars) for (int i = 0; i < 12; ++i) scalars[i] = s[i];
+        return 0;
+    } catch (const std::exception& e) { flush_counters(); set_err(err, errlen, e.what()); return 1; }
+}
 static const Pts* grid_sel(OrcGrids* g, int which) {
     switch (which) {
         case 0: return &g->g.star1f; case 1: return &g->g.star2f; case 2: return &g->g.star1c; case 3: return &g->g.star2c;

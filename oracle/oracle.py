@@ -30,6 +30,39 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
+def host_cpu() -> str:
+    """Model name of this host's CPU (/proc/cpuinfo)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def use_native() -> str:
+    """Switches this process to the oracle built for the host's own CPU
+    (-O3 -march=native, no FMA contraction: the same results), building it on
+    first use; the timed CPU baseline runs it.  Must come before the first
+    lib() call.  Returns the library path."""
+    global LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("use_native() must be called before the oracle is loaded")
+    import hashlib
+    flags = ""
+    try:
+        flags = next((ln for ln in open("/proc/cpuinfo") if ln.startswith("flags")), "")
+    except OSError:
+        pass
+    key = hashlib.sha1((host_cpu() + flags).encode()).hexdigest()[:12]
+    so = HERE / "_native" / f"liblcurve_oracle_{key}.so"
+    if not so.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_SO=_native/{so.name}"], check=True)
+    LIB_PATH = so
+    return str(so)
+
+
 def lib():
     global _lib
     if _lib is not None:
@@ -57,6 +90,8 @@ def lib():
     L.orc_grids_fetch.argtypes = [vp, ip, dp, dp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                   C.POINTER(C.c_float), C.POINTER(C.c_int), dp]
     L.orc_grids_info.argtypes = [vp, dp]
+    L.orc_grids_light_curve.argtypes = [vp, vp, vp, ip, ip, ip, ip, dp, dp, cp, ip]
+    L.orc_set_grid_threads.argtypes = [ip]
     for f in ("orc_xl1",):
         getattr(L, f).argtypes = [C.c_double]
         getattr(L, f).restype = C.c_double
@@ -90,6 +125,14 @@ def _dp(a: np.ndarray):
 
 class OracleError(RuntimeError):
     pass
+
+
+def _lc_dict(calc, sc):
+    keys = ["wdwarf", "chisq", "wnok", "logg1", "logg2", "rv1", "rv2"]
+    out = {k: sc[i] for i, k in enumerate(keys)}
+    out["sfac"] = sc[7:12].copy()
+    out["calc"] = calc
+    return out
 
 
 def make_data(times, expose=0.001, ndiv=1, flux=0.0, ferr=1.0, weight=1.0) -> np.ndarray:
@@ -155,11 +198,7 @@ class Model:
                                    _dp(calc), _dp(sc), err, 512)
         if rc != 0:
             raise OracleError(err.value.decode())
-        keys = ["wdwarf", "chisq", "wnok", "logg1", "logg2", "rv1", "rv2"]
-        out = {k: sc[i] for i, k in enumerate(keys)}
-        out["sfac"] = sc[7:12].copy()
-        out["calc"] = calc
-        return out
+        return _lc_dict(calc, sc)
 
     def chisq_batch(self, data: np.ndarray, names, values, scale=False, nthreads=1) -> np.ndarray:
         data = np.ascontiguousarray(data, dtype=DATUM_DTYPE)
@@ -173,30 +212,71 @@ class Model:
         return out
 
     def grids(self):
-        g = C.c_void_p()
+        return self.built_grids().fetch_all()
+
+    def built_grids(self, threads: int = 1) -> "Grids":
+        """The model's grids (orchestration.rs:36-170), kept for fetching and for
+        light curves on them.  threads > 1 computes the elements' eclipse
+        intervals with that many threads (same values; for large grids)."""
+        return Grids(self, threads)
+
+
+class Grids:
+    """Handle of the oracle's grids of one model (built once)."""
+
+    def __init__(self, model: Model, threads: int = 1):
+        self.model = model
+        self._g = C.c_void_p()
         err = C.create_string_buffer(512)
-        if lib().orc_grids_build(self._h, C.byref(g), err, 512) != 0:
-            raise OracleError(err.value.decode())
+        lib().orc_set_grid_threads(int(threads))
         try:
-            out = {}
-            for name, w in GRID_NAMES.items():
-                n = lib().orc_grids_count(g, w)
-                posn = np.zeros((n, 3)); dirn = np.zeros((n, 3))
-                area = np.zeros(n, np.float32); grav = np.zeros(n, np.float32); flux = np.zeros(n, np.float32)
-                necl = np.zeros(n, np.int32); ecl = np.zeros((n, 8))
-                lib().orc_grids_fetch(g, w, _dp(posn), _dp(dirn),
-                                      area.ctypes.data_as(C.POINTER(C.c_float)),
-                                      grav.ctypes.data_as(C.POINTER(C.c_float)),
-                                      flux.ctypes.data_as(C.POINTER(C.c_float)),
-                                      necl.ctypes.data_as(C.POINTER(C.c_int)), _dp(ecl))
-                out[name] = dict(posn=posn, dirn=dirn, area=area, gravity=grav, flux=flux, necl=necl, ecl=ecl)
-            info = np.zeros(10)
-            lib().orc_grids_info(g, _dp(info))
-            out["info"] = dict(phase1=info[0], phase2=info[1], scale11=info[2], scale12=info[3],
-                               scale21=info[4], scale22=info[5], rlens1=info[6], bspot=info[7:10].copy())
-            return out
+            rc = lib().orc_grids_build(model._h, C.byref(self._g), err, 512)
         finally:
-            lib().orc_grids_free(g)
+            lib().orc_set_grid_threads(1)
+        if rc != 0:
+            raise OracleError(err.value.decode())
+
+    def __del__(self):
+        if getattr(self, "_g", None) and _lib is not None:
+            _lib.orc_grids_free(self._g)
+            self._g = None
+
+    def fetch(self, name: str):
+        g, w = self._g, GRID_NAMES[name]
+        n = lib().orc_grids_count(g, w)
+        posn = np.zeros((n, 3)); dirn = np.zeros((n, 3))
+        area = np.zeros(n, np.float32); grav = np.zeros(n, np.float32); flux = np.zeros(n, np.float32)
+        necl = np.zeros(n, np.int32); ecl = np.zeros((n, 8))
+        lib().orc_grids_fetch(g, w, _dp(posn), _dp(dirn),
+                              area.ctypes.data_as(C.POINTER(C.c_float)),
+                              grav.ctypes.data_as(C.POINTER(C.c_float)),
+                              flux.ctypes.data_as(C.POINTER(C.c_float)),
+                              necl.ctypes.data_as(C.POINTER(C.c_int)), _dp(ecl))
+        return dict(posn=posn, dirn=dirn, area=area, gravity=grav, flux=flux, necl=necl, ecl=ecl)
+
+    def info(self):
+        info = np.zeros(10)
+        lib().orc_grids_info(self._g, _dp(info))
+        return dict(phase1=info[0], phase2=info[1], scale11=info[2], scale12=info[3],
+                    scale21=info[4], scale22=info[5], rlens1=info[6], bspot=info[7:10].copy())
+
+    def fetch_all(self):
+        out = {name: self.fetch(name) for name in GRID_NAMES}
+        out["info"] = self.info()
+        return out
+
+    def light_curve(self, data: np.ndarray, scale=False, rdata=False, nthreads=1):
+        """light_curve on these grids (the time loop onwards, orchestration.rs:171-318)."""
+        data = np.ascontiguousarray(data, dtype=DATUM_DTYPE)
+        n = data.shape[0]
+        calc = np.zeros(n)
+        sc = np.zeros(12)
+        err = C.create_string_buffer(512)
+        rc = lib().orc_grids_light_curve(self._g, self.model._h, data.ctypes.data, n, int(scale), int(rdata),
+                                         int(nthreads), _dp(calc), _dp(sc), err, 512)
+        if rc != 0:
+            raise OracleError(err.value.decode())
+        return _lc_dict(calc, sc)
 
 
 def chisq_ragged(models, data: np.ndarray, offsets, scale=False, nthreads=1) -> np.ndarray:

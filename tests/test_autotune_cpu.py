@@ -74,3 +74,16 @@ def test_batches_without_roche_elements_skip_that_axis(A):
     b.set_tuning = spy
     A.autotune(b)
     assert all(args[1] in (0, FakeBatch.HEURISTIC["roche_split"]) for args in seen)
+
+
+def test_unsearched_axis_is_cached_as_the_heuristic(A, tmp_path):
+    # a batch without Roche-eclipsed elements never times the scan split: the cache keeps 0
+    # (the planner's heuristic) for it, so the choice cannot pin a later batch that has them
+    cache = tmp_path / "tune.json"
+    A.autotune(FakeBatch(roche=0), cache=cache, device_name="B200")
+    (choice,) = json.loads(cache.read_text())["B200"].values()
+    assert choice["roche_split"] == 0
+    later = FakeBatch(roche=0)
+    later.t["roche_split"] = 16
+    assert A.apply_cached(later, cache, device_name="B200")
+    assert later.tuning()["roche_split"] == FakeBatch.HEURISTIC["roche_split"]

@@ -85,3 +85,31 @@ def test_roche_search_counts_and_skips(lcb, oracle, W):
         oracle.Model(text=text).light_curve(data[lo:hi], nthreads=1)
     ref = oracle.counters()["fblink"]
     assert c["searches"] == ref, (c, ref)
+
+
+def test_diag_identities_on_gpu_grids(lcb, oracle, W):
+    """crates/lcurve/examples/diag.rs:31-55 on the GPU's grids: the spherical
+    star's area and flux sums approach 4 pi r1^2 and planck(550, t1) 4 pi r1^2
+    at second order, and equal the oracle's sums to f32 rounding; the Roche
+    secondary's area converges at second order too."""
+    import math
+    from test_oracle_golden import _sphere_text, sphere_sums
+    r1, t1 = 0.015, 15000.0
+    exact = 4.0 * math.pi * r1 * r1
+    bb = oracle.lib().orc_planck(550.0, t1)
+    errs = []
+    for nlat in (20, 50, 100, 200):
+        text = _sphere_text(nlat, W)
+        area, flux = sphere_sums(lcb.Model(text=text).grid("star1f"))
+        oarea, oflux = sphere_sums(oracle.Model(text=text).grids()["star1f"])
+        assert area == pytest.approx(oarea, rel=1e-6) and flux == pytest.approx(oflux, rel=1e-6)
+        assert abs(flux / (bb * area) - 1.0) < 1e-6
+        errs.append(abs(area / exact - 1.0))
+        assert errs[-1] < 0.1 * (math.pi / nlat) ** 2
+    assert errs == sorted(errs, reverse=True) and 2.5 < errs[1] / errs[2] < 6.0
+    areas = []
+    for nlat in (50, 100, 200):
+        text = W.model_text(nlat1f=10, nlat1c=10, nlat2f=nlat, nlat2c=nlat, eclipse1=0, eclipse2=0)
+        areas.append(sphere_sums(lcb.Model(text=text).grid("star2f"))[0])
+    d1, d2 = areas[1] - areas[0], areas[2] - areas[1]
+    assert 2.5 < d1 / d2 < 6.0, areas

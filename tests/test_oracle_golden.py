@@ -218,3 +218,50 @@ def test_numerical_known_answers(oracle):
     yx = (C.c_double * 2)()
     L.orc_bsstep_exp(yx)
     assert yx[1] > 0.0 and abs(yx[0] - math.exp(yx[1])) / math.exp(yx[1]) < 1e-8
+
+
+# ---- crates/lcurve/examples/diag.rs:31-55: grid and continuum identities ----
+def _sphere_text(nlat, W):
+    # the golden model's spherical white dwarf (roche1 = 0, r1 = 0.015); absorb = 0: no
+    # irradiation, so each element's flux is its area times planck(wavelength, t1); eclipses off
+    # (they change no area or flux)
+    return W.model_text(nlat1f=nlat, nlat1c=nlat, nlat2f=10, nlat2c=10, absorb=0.0, eclipse1=0, eclipse2=0)
+
+
+def sphere_sums(g):
+    return float(np.sum(g["area"].astype(np.float64))), float(np.sum(g["flux"].astype(np.float64)))
+
+
+def test_diag_sphere_area_and_flux_identities(oracle):
+    """Sum of star 1's element areas -> 4 pi r1^2 and sum of fluxes -> planck(550 nm, t1)
+    4 pi r1^2 (diag.rs:34-55); the latitude bands are a midpoint rule in theta, so the
+    relative error is about (pi / nlat)^2 / 24 and falls as 1 / nlat^2."""
+    import importlib
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    r1, t1 = 0.015, 15000.0
+    exact = 4.0 * math.pi * r1 * r1
+    bb = oracle.lib().orc_planck(550.0, t1)
+    errs = []
+    for nlat in (20, 50, 100, 200):
+        area, flux = sphere_sums(oracle.Model(text=_sphere_text(nlat, W)).grids()["star1f"])
+        e = area / exact - 1.0
+        assert abs(e) < 0.1 * (math.pi / nlat) ** 2, (nlat, e)
+        assert abs(flux / (bb * area) - 1.0) < 1e-6  # per element f32 rounding only
+        assert abs(flux / (bb * exact) - 1.0) < 0.1 * (math.pi / nlat) ** 2
+        errs.append(abs(e))
+    assert errs == sorted(errs, reverse=True)
+    assert 2.5 < errs[1] / errs[2] < 6.0  # second order: halving the spacing quarters the error
+
+
+def test_diag_roche_star_area_converges(oracle):
+    """The Roche-lobe-filling secondary's area at nlat 50/100/200 converges at
+    second order (successive differences shrink about four-fold)."""
+    import importlib
+    W = importlib.import_module("lcurve-rs_b200.workloads")
+    areas = []
+    for nlat in (50, 100, 200):
+        text = W.model_text(nlat1f=10, nlat1c=10, nlat2f=nlat, nlat2c=nlat, eclipse1=0, eclipse2=0)
+        areas.append(sphere_sums(oracle.Model(text=text).grids()["star2f"])[0])
+    d1, d2 = areas[1] - areas[0], areas[2] - areas[1]
+    assert abs(d2) < abs(d1)
+    assert 2.5 < d1 / d2 < 6.0, (areas, d1, d2)

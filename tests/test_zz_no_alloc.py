@@ -92,3 +92,66 @@ def test_noalloc_rejects_a_model_beyond_the_arena(lcb, W):
     rc, calc, res = _call(lcb, "lcb_light_curve_noalloc", m, da, False)
     lcb._capi.check(rc)
     _assert_same(res, calc, ref_res, ref_calc, False)
+
+
+def test_noalloc_allocates_no_device_memory(lcb, W):
+    import torch
+    m, d, scale = _cases(lcb, W)[1]
+    rc, ref_calc, ref_res = _call(lcb, "lcb_light_curve", m, d, scale)
+    lcb._capi.check(rc)
+    lcb._capi.check(_call(lcb, "lcb_light_curve_noalloc", m, d, scale)[0])  # warm: every kernel launched once
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc, calc, res = _call(lcb, "lcb_light_curve_noalloc", m, d, scale)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    lcb._capi.check(rc)
+    assert free1 == free0
+    _assert_same(res, calc, ref_res, ref_calc, scale)
+
+
+def test_noalloc_calls_from_two_threads(lcb, W):
+    """Two host threads, each with its own context on the same device, call the
+    entry point at once: the calls share the arena, so the library must run
+    them one at a time, and every result must still match."""
+    import threading
+
+    L = lcb._capi.load()
+    cases = _cases(lcb, W)[:2]
+    refs = []
+    for m, d, scale in cases:
+        rc, calc, res = _call(lcb, "lcb_light_curve", m, d, scale)
+        lcb._capi.check(rc)
+        refs.append((calc, res))
+    dev = int(str(lcb.get_device()).split(":")[-1]) if ":" in str(lcb.get_device()) else 0
+    ctxs = []
+    for _ in range(2):
+        h = C.c_void_p()
+        lcb._capi.check(L.lcb_ctx_create(dev, C.byref(h)))
+        ctxs.append(h)
+    errors = []
+
+    def worker(k):
+        m, d, scale = cases[k]
+        ref_calc, ref_res = refs[k]
+        try:
+            for _ in range(4):
+                calc = np.zeros(d.shape[0])
+                res = lcb.Result()
+                rc = L.lcb_light_curve_noalloc(ctxs[k], m._h, d.ctypes.data, d.shape[0], int(scale), 0,
+                                               lcb._capi.dptr(calc), C.byref(res))
+                assert rc == 0, rc
+                _assert_same(res, calc, ref_res, ref_calc, scale)
+        except BaseException as e:  # noqa: BLE001 (reported by the main thread)
+            errors.append(e)
+
+    try:
+        threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+    finally:
+        for h in ctxs:
+            L.lcb_ctx_destroy(h)
+    assert not errors, errors
