@@ -46,6 +46,14 @@ int  lcb_mlp_num_params(const lcb_mlp* net, int64_t* n);
 int  lcb_mlp_get_params(lcb_mlp* net, float* host, int64_t n);
 int  lcb_mlp_set_params(lcb_mlp* net, const float* host, int64_t n);
 int  lcb_mlp_get_grads(lcb_mlp* net, float* host, int64_t n);
+/* Training state for checkpoint / resume: FP32 master parameters and the two
+ * Adam moments, each state_size floats in the network's own (padded) device
+ * layout, concatenated (3 x state_size), plus the Adam step count.  Valid for
+ * a network of the same shape; set_state also refreshes the BF16 weights, so
+ * training resumes exactly where get_state left it (synchronise). */
+int  lcb_mlp_state_size(const lcb_mlp* net, int64_t* n);
+int  lcb_mlp_get_state(lcb_mlp* net, float* host, int64_t n, int64_t* steps);
+int  lcb_mlp_set_state(lcb_mlp* net, const float* host, int64_t n, int64_t steps);
 
 /* y_dev[batch x n_out] = net(x_dev[batch x n_in]) (fp32 in and out). */
 int  lcb_mlp_forward(lcb_mlp* net, const float* x_dev, int64_t batch, float* y_dev);

@@ -51,7 +51,8 @@ SYMBOLS = [
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
     "lcb_mlp_train_step", "lcb_mlp_grads_device", "lcb_mlp_adam_step", "lcb_mlp_take_loss", "lcb_mlp_sync",
-    "lcb_mlp_gemm", "lcb_logflux_chisq", "lcb_surrogate_subchain",
+    "lcb_mlp_gemm", "lcb_logflux_chisq", "lcb_surrogate_subchain", "lcb_mlp_state_size", "lcb_mlp_get_state",
+    "lcb_mlp_set_state",
 ]
 
 _lib = None
@@ -109,6 +110,9 @@ def load():
         "lcb_mlp_get_params": ([vp, vp, i64], i),
         "lcb_mlp_set_params": ([vp, vp, i64], i),
         "lcb_mlp_get_grads": ([vp, vp, i64], i),
+        "lcb_mlp_state_size": ([vp, i64p], i),
+        "lcb_mlp_get_state": ([vp, vp, i64, i64p], i),
+        "lcb_mlp_set_state": ([vp, vp, i64, i64], i),
         "lcb_mlp_forward": ([vp, vp, i64, vp], i),
         "lcb_mlp_backward": ([vp, vp, vp, i64], i),
         "lcb_mlp_train_step": ([vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float], i),

@@ -1099,6 +1099,44 @@ int lcb_mlp_get_params(lcb_mlp* net, float* host, int64_t n) {
     return fetch_flat(net, net->p.p, host, n);
 }
 
+// Training state for checkpoints: the FP32 master parameters and both Adam
+// moments in the device layout (3 x state_size floats) and the step count.
+int lcb_mlp_state_size(const lcb_mlp* net, int64_t* n) {
+    if (!net || !n) return LCB_ERR_INVALID;
+    *n = net->nparam;
+    return LCB_OK;
+}
+
+int lcb_mlp_get_state(lcb_mlp* net, float* host, int64_t n, int64_t* steps) {
+    if (!net || !host || !steps) return LCB_ERR_INVALID;
+    return guard([&] {
+        if (n != 3 * net->nparam) throw Fail(LCB_ERR_INVALID, "state size mismatch");
+        CK(cudaSetDevice(net->device));
+        net->check_err();
+        const size_t b = net->nparam * sizeof(float);
+        CK(cudaMemcpyAsync(host, net->p.p, b, cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaMemcpyAsync(host + net->nparam, net->m.p, b, cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaMemcpyAsync(host + 2 * net->nparam, net->v.p, b, cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaStreamSynchronize(net->stream));
+        *steps = net->steps;
+    });
+}
+
+int lcb_mlp_set_state(lcb_mlp* net, const float* host, int64_t n, int64_t steps) {
+    if (!net || !host || steps < 0) return LCB_ERR_INVALID;
+    return guard([&] {
+        if (n != 3 * net->nparam) throw Fail(LCB_ERR_INVALID, "state size mismatch");
+        CK(cudaSetDevice(net->device));
+        const size_t b = net->nparam * sizeof(float);
+        CK(cudaMemcpyAsync(net->p.p, host, b, cudaMemcpyHostToDevice, net->stream));
+        CK(cudaMemcpyAsync(net->m.p, host + net->nparam, b, cudaMemcpyHostToDevice, net->stream));
+        CK(cudaMemcpyAsync(net->v.p, host + 2 * net->nparam, b, cudaMemcpyHostToDevice, net->stream));
+        net->steps = steps;
+        net->refresh_bf16();
+        CK(cudaStreamSynchronize(net->stream));
+    });
+}
+
 int lcb_mlp_get_grads(lcb_mlp* net, float* host, int64_t n) {
     if (!net || !host) return LCB_ERR_INVALID;
     return fetch_flat(net, net->g.p, host, n);

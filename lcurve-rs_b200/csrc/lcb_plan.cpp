@@ -12,11 +12,14 @@
 #include "lcb_plan.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 
 namespace lcb {
 
@@ -306,28 +309,48 @@ void stream_to_radius_uncached(double q, double rad, double out[3]) {
 // stream_to_radius_uncached memoised on (q, rad), process-wide: the integration is ~20,000
 // serial right-hand-side evaluations (the reference's 1e-3 step cap), and fits, batches and
 // repeated light curves mostly revisit the same geometry.  The result is a function of (q, rad)
-// alone, so a hit returns exactly what the integration would; failures are not cached.
+// alone, so a hit returns exactly what the integration would; failures are not cached.  The
+// table holds the last kSpotMemo distinct pairs, enough for every model of a large batch
+// (plan_batch integrates a batch's new pairs in parallel first, then every model hits).
+constexpr size_t kSpotMemo = 8192;
+struct SpotKey {
+    uint64_t q, rad;
+    bool operator==(const SpotKey& o) const { return q == o.q && rad == o.rad; }
+};
+struct SpotKeyHash {
+    size_t operator()(const SpotKey& k) const { return (size_t)(k.q * 0x9E3779B97F4A7C15ull ^ (k.rad + (k.q >> 7))); }
+};
+static std::mutex g_spot_mu;
+static std::unordered_map<SpotKey, std::array<double, 3>, SpotKeyHash> g_spot_memo;
+static std::deque<SpotKey> g_spot_order;
+
+static SpotKey spot_key(double q, double rad) {
+    SpotKey k;
+    std::memcpy(&k.q, &q, 8);
+    std::memcpy(&k.rad, &rad, 8);
+    return k;
+}
+
+static bool spot_cached(double q, double rad, double out[3]) {
+    std::lock_guard<std::mutex> g(g_spot_mu);
+    auto it = g_spot_memo.find(spot_key(q, rad));
+    if (it == g_spot_memo.end()) return false;
+    out[0] = it->second[0]; out[1] = it->second[1]; out[2] = it->second[2];
+    return true;
+}
+
 void stream_to_radius(double q, double rad, double out[3]) {
-    struct Entry {
-        double q, rad, xyz[3];
-        bool used;
-    };
-    constexpr int kEntries = 64;
-    static std::mutex mu;
-    static Entry cache[kEntries] = {};
-    static int next = 0;
-    {
-        std::lock_guard<std::mutex> g(mu);
-        for (const Entry& e : cache)
-            if (e.used && e.q == q && e.rad == rad) {
-                out[0] = e.xyz[0]; out[1] = e.xyz[1]; out[2] = e.xyz[2];
-                return;
-            }
-    }
+    if (spot_cached(q, rad, out)) return;
     stream_to_radius_uncached(q, rad, out);
-    std::lock_guard<std::mutex> g(mu);
-    cache[next] = Entry{q, rad, {out[0], out[1], out[2]}, true};
-    next = (next + 1) % kEntries;
+    std::lock_guard<std::mutex> g(g_spot_mu);
+    const SpotKey k = spot_key(q, rad);
+    if (g_spot_memo.emplace(k, std::array<double, 3>{out[0], out[1], out[2]}).second) {
+        g_spot_order.push_back(k);
+        if (g_spot_order.size() > kSpotMemo) {
+            g_spot_memo.erase(g_spot_order.front());
+            g_spot_order.pop_front();
+        }
+    }
 }
 
 // Latitude bands of one star grid (grid.rs:157-322) appended to `bands`;
@@ -763,6 +786,27 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             lay[i].dev.status = -1;
         }
     };
+    // a bright spot's stream integration (~0.7 ms) outweighs the rest of a model's planning:
+    // the batch's pairs (q, radius_spot) missing from the memo are integrated first, one per
+    // thread, so that a small batch (an MCMC step over q) does not run them eight to a thread
+    {
+        std::vector<std::pair<double, double>> need;
+        for (int64_t i = 0; i < n; ++i) {
+            const Model& m = *models[i];
+            double o[3];
+            if (m.add_spot && count[i] > 0 && !spot_cached(m.v(P_Q), m.v(P_RADIUS_SPOT), o))
+                need.emplace_back(m.v(P_Q), m.v(P_RADIUS_SPOT));
+        }
+        std::sort(need.begin(), need.end());
+        need.erase(std::unique(need.begin(), need.end()), need.end());
+        parallel_for((int64_t)need.size(), 1, [&](int64_t k) {
+            double o[3];
+            try {
+                stream_to_radius(need[k].first, need[k].second, o);
+            } catch (const std::exception&) {  // the model's own planning reports it
+            }
+        });
+    }
     // models are independent: prepare them on the host's cores (8 or more per thread)
     parallel_for(n, 8, prep);
     // sub-phases and data: per-model sums, prefix offsets, then the per-datum

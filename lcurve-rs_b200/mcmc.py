@@ -167,6 +167,39 @@ class Run:
         return self.accepted / max(self.proposals, 1)
 
 
+class Checkpoint:
+    """Sampler state saved every `every` steps to `path` (.npz: positions, log
+    probabilities, the chain so far, counters, elapsed seconds and the random
+    generator's state), from which a run resumes exactly: the resumed chain is
+    the uninterrupted one, step for step and bit for bit.  The reference's
+    fitter keeps its emcee chains in memory only (python/lcurve_rs/
+    fitting.py:590-601)."""
+
+    def __init__(self, path, every: int):
+        import pathlib  # noqa: PLC0415
+        self.path = pathlib.Path(path)
+        self.every = int(every)
+
+    def due(self, step: int) -> bool:
+        return self.every > 0 and (step + 1) % self.every == 0
+
+    def save(self, rng, step: int, chain: np.ndarray, seconds: float, **arrays) -> None:
+        import json  # noqa: PLC0415
+        tmp = self.path.with_name(self.path.name + ".tmp.npz")
+        np.savez(tmp, step=step, chain=chain[:step], seconds=seconds,
+                 rng=np.array(json.dumps(rng.bit_generator.state)), **arrays)
+        tmp.replace(self.path)
+
+    def load(self):
+        """(step, chain prefix, seconds, rng state, other arrays) or None."""
+        import json  # noqa: PLC0415
+        if not self.path.exists():
+            return None
+        with np.load(self.path) as z:
+            other = {k: z[k] for k in z.files if k not in ("step", "chain", "seconds", "rng")}
+            return int(z["step"]), z["chain"], float(z["seconds"]), json.loads(str(z["rng"])), other
+
+
 def shard_bounds(n: int, world: int) -> list[int]:
     """Row r of n belongs to rank k when bounds[k] <= r < bounds[k + 1]."""
     return [k * n // world for k in range(world + 1)]
@@ -209,7 +242,10 @@ def _eval_prob(engine, theta, group=None):
 
 
 def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0, move: str = "stretch",
-              bandwidth: float = 1.0, group=None) -> Run:
+              bandwidth: float = 1.0, group=None, checkpoint: Checkpoint | None = None) -> Run:
+    """The plain sampler; with `checkpoint`, its state is saved every
+    checkpoint.every steps and a run whose checkpoint file exists resumes
+    from it."""
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -217,9 +253,18 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
     chain = np.empty((nsteps, nw, d))
     t0 = time.perf_counter()
     ev0 = engine.evals
-    lp = _eval_prob(engine, x, group)
-    acc = props = 0
-    for s in range(nsteps):
+    acc = props = first = 0
+    state = checkpoint.load() if checkpoint else None
+    if state is not None:
+        first, prefix, done_s, rng.bit_generator.state, o = state
+        chain[:first] = prefix
+        x, lp = o["x"].copy(), o["lp"].copy()
+        acc, props = int(o["counts"][0]), int(o["counts"][1])
+        ev0 -= int(o["counts"][2])
+        t0 -= done_s
+    else:
+        lp = _eval_prob(engine, x, group)
+    for s in range(first, nsteps):
         perm = rng.permutation(nw)
         for h in (0, 1):
             S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
@@ -238,12 +283,16 @@ def run_plain(engine, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0
             acc += int(take.sum())
             props += len(S)
         chain[s] = x
+        if checkpoint and checkpoint.due(s):
+            checkpoint.save(rng, s + 1, chain, time.perf_counter() - t0, x=x, lp=lp,
+                            counts=np.array([acc, props, engine.evals - ev0]))
     return Run(chain, time.perf_counter() - t0, engine.evals - ev0, proposals=props, accepted=acc)
 
 
 def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a: float = 2.0,
                 substeps: int = 1, device_subchain: bool | None = None, move: str = "stretch",
-                bandwidth: float = 1.0, group=None) -> Run:
+                bandwidth: float = 1.0, group=None, checkpoint: Checkpoint | None = None) -> Run:
+    """The delayed-acceptance sampler; `checkpoint` as in run_plain."""
     rng = np.random.default_rng(seed)
     x = np.array(p0, dtype=np.float64)
     nw, d = x.shape
@@ -251,11 +300,20 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
     chain = np.empty((nsteps, nw, d))
     t0 = time.perf_counter()
     ev0 = engine.evals
-    lp = _eval_prob(engine, x, group)
-    lps = log_prior(x) + _loglike(surrogate.chisq(x, scale=True))
     on_device = hasattr(surrogate, "subchain") if device_subchain is None else device_subchain
-    acc = props = passed = nsur = 0
-    for s in range(nsteps):
+    acc = props = passed = nsur = first = 0
+    state = checkpoint.load() if checkpoint else None
+    if state is not None:
+        first, prefix, done_s, rng.bit_generator.state, o = state
+        chain[:first] = prefix
+        x, lp, lps = o["x"].copy(), o["lp"].copy(), o["lps"].copy()
+        acc, props, passed, nsur = (int(v) for v in o["counts"][:4])
+        ev0 -= int(o["counts"][4])
+        t0 -= done_s
+    else:
+        lp = _eval_prob(engine, x, group)
+        lps = log_prior(x) + _loglike(surrogate.chisq(x, scale=True))
+    for s in range(first, nsteps):
         perm = rng.permutation(nw)
         for h in (0, 1):
             S, Cc = (perm[:half], perm[half:]) if h == 0 else (perm[half:], perm[:half])
@@ -281,6 +339,9 @@ def run_delayed(engine, surrogate, p0: np.ndarray, nsteps: int, seed: int = 0, a
                 passed += len(idx)
             props += len(S)
         chain[s] = x
+        if checkpoint and checkpoint.due(s):
+            checkpoint.save(rng, s + 1, chain, time.perf_counter() - t0, x=x, lp=lp, lps=lps,
+                            counts=np.array([acc, props, passed, nsur, engine.evals - ev0]))
     return Run(chain, time.perf_counter() - t0, engine.evals - ev0, surrogate_evals=nsur, stage1_pass=passed,
                proposals=props, accepted=acc)
 

@@ -210,7 +210,7 @@ class Surrogate:
         return torch.as_tensor(x).to(self.dev)
 
     def fit(self, theta: np.ndarray, flux: np.ndarray, epochs: int = 60, batch: int = 8192, lr: float = 2e-3,
-            lr_min: float = 2e-5, log=None, group=None) -> list[float]:
+            lr_min: float = 2e-5, log=None, group=None, renormalize: bool = True) -> list[float]:
         """Trains on (theta, flux) rows with finite fluxes; cosine learning-rate
         schedule, Adam.  Returns the mean training loss of each epoch.
 
@@ -235,9 +235,11 @@ class Surrogate:
         with torch.cuda.stream(self._stream):
             logf = torch.as_tensor(_shape(flux), dtype=torch.float32).to(self.dev)
             # one scale for every phase: the loss is then the mean squared
-            # log-flux error, the quantity the chi-squared weighs uniformly
-            self.mean = logf.mean(dim=0)
-            self.sd = torch.full_like(self.mean, float((logf - self.mean).std().clamp_min(1e-6)))
+            # log-flux error, the quantity the chi-squared weighs uniformly;
+            # a further fit (renormalize=False) keeps the trained network's scale
+            if renormalize:
+                self.mean = logf.mean(dim=0)
+                self.sd = torch.full_like(self.mean, float((logf - self.mean).std().clamp_min(1e-6)))
             Y = ((logf - self.mean) / self.sd).contiguous()
             X = self._x(theta)
         self._stream.synchronize()
@@ -282,6 +284,34 @@ class Surrogate:
                 log(f"epoch {ep} loss {losses[-1]:.3e} ({time.perf_counter() - t0:.1f} s)")
         self.train_seconds += time.perf_counter() - t0
         return losses
+
+    def save(self, path) -> None:
+        """Checkpoint (.npz): the network's shape, its training state (FP32
+        parameters, Adam moments and step count), the output normalisation and
+        the training time so far.  Surrogate.load resumes training exactly."""
+        n = C.c_int64()
+        _capi.check_mlp(self.L.lcb_mlp_state_size(self._h, C.byref(n)))
+        state = np.empty(3 * n.value, dtype=np.float32)
+        steps = C.c_int64()
+        _capi.check_mlp(self.L.lcb_mlp_get_state(self._h, C.c_void_p(state.ctypes.data), state.size,
+                                                 C.byref(steps)))
+        np.savez(path, state=state, steps=steps.value, mean=self.mean.cpu().numpy(), sd=self.sd.cpu().numpy(),
+                 shape=np.array([self.n_phase, self.width, self.n_hidden, self.max_batch]),
+                 train_seconds=self.train_seconds)
+
+    @classmethod
+    def load(cls, path, device: int = 0) -> "Surrogate":
+        torch = _torch()
+        with np.load(path) as z:
+            n_phase, width, n_hidden, max_batch = (int(v) for v in z["shape"])
+            sur = cls(n_phase=n_phase, width=width, n_hidden=n_hidden, max_batch=max_batch, device=device)
+            state = np.ascontiguousarray(z["state"], dtype=np.float32)
+            _capi.check_mlp(sur.L.lcb_mlp_set_state(sur._h, C.c_void_p(state.ctypes.data), state.size,
+                                                    int(z["steps"])))
+            sur.mean = torch.as_tensor(z["mean"]).to(sur.dev)
+            sur.sd = torch.as_tensor(z["sd"]).to(sur.dev)
+            sur.train_seconds = float(z["train_seconds"])
+        return sur
 
     def _grads_tensor(self):
         """The network's device gradient buffer as a torch tensor (no copy)."""
@@ -391,3 +421,28 @@ class Surrogate:
             self._stage_d = torch.empty(self._stage_n, dtype=torch.float64, device=self.dev)
             self._out_h = torch.empty(self._stage_n, dtype=torch.float64, pin_memory=True)
         return self._stage_h, self._stage_d
+
+
+def refine_near(sur: Surrogate, setup: CurveSetup, ensemble: np.ndarray, theta_global: np.ndarray,
+                flux_global: np.ndarray, n: int = 131072, widen: float = 3.0, epochs: int = 40, seed: int = 7,
+                lr: float = 5e-4, log=None) -> float:
+    """Sharpens the surrogate where a sampler's ensemble sits: n parameter
+    rows drawn from a Gaussian with the ensemble's mean and covariance widened
+    by `widen` (kept inside the prior box), their curves computed by the
+    engine, and `epochs` further epochs of training on them mixed with as
+    many rows of the global training set (so the rest of the box is kept).
+    The sampler that uses the surrogate afterwards stays exact: delayed
+    acceptance corrects any surrogate error, a better surrogate only wastes
+    fewer engine evaluations.  Returns the seconds spent (curves + training)."""
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    mu = ensemble.mean(axis=0)
+    cov = np.cov(ensemble, rowvar=False) * widen ** 2 + np.diag(1e-12 * (PRIOR_HI - PRIOR_LO) ** 2)
+    local = rng.multivariate_normal(mu, cov, size=2 * n)
+    local = local[np.all((local >= PRIOR_LO) & (local <= PRIOR_HI), axis=1)][:n]
+    curves = generate_curves(setup, local)
+    pick = rng.choice(theta_global.shape[0], size=min(n, theta_global.shape[0]), replace=False)
+    theta = np.concatenate([local, theta_global[pick]])
+    flux = np.concatenate([curves, flux_global[pick]])
+    sur.fit(theta, flux, epochs=epochs, lr=lr, lr_min=lr * 0.01, log=log, renormalize=False)
+    return time.perf_counter() - t0

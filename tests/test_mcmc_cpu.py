@@ -141,3 +141,28 @@ def test_sharded_engine_evaluations_give_the_single_process_chains():
         assert np.array_equal(out[r][0], single[0]) and np.array_equal(out[r][1], single[1])
     assert out[0][2] + out[1][2] == single[2] and out[0][3] + out[1][3] == single[3]
     assert 0 < out[0][2] < single[2]
+
+
+@pytest.mark.parametrize("sampler", ["plain", "delayed"])
+def test_checkpoint_resume_reproduces_the_uninterrupted_chain(M, S, tmp_path, sampler):
+    """A run stopped after its checkpoint and resumed from it gives the
+    uninterrupted run's chain bit for bit (same positions, counters)."""
+    mu = 0.5 * (S.PRIOR_LO + S.PRIOR_HI)
+    p0 = M.initial_walkers(32, mu, seed=1, spread=0.02)
+
+    def run(nsteps, ck=None):
+        eng = Gaussian(S, mu, 0.02)
+        if sampler == "plain":
+            return M.run_plain(eng, p0, nsteps, seed=9, move="kde", checkpoint=ck)
+        return M.run_delayed(eng, Gaussian(S, mu, 0.03, shift=0.5), p0, nsteps, seed=9, substeps=3, move="kde",
+                             checkpoint=ck)
+
+    full = run(60)
+    ck = M.Checkpoint(tmp_path / "chain.npz", every=25)
+    run(25, ck)   # "interrupted" after its checkpoint at step 25
+    assert ck.path.exists()
+    resumed = run(60, M.Checkpoint(ck.path, every=0))
+    assert np.array_equal(resumed.chain, full.chain)
+    assert (resumed.accepted, resumed.proposals, resumed.engine_evals) == \
+           (full.accepted, full.proposals, full.engine_evals)
+    assert resumed.stage1_pass == full.stage1_pass and resumed.surrogate_evals == full.surrogate_evals
