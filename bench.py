@@ -213,6 +213,36 @@ def traffic_from_profiles(kernel):
         return None
 
 
+def spot_stream_timing(lcb, specs, data, offs, steps=3):
+    """Wall-clock ms of lcb_chisq_batch_ragged on these models with a bright
+    spot (add_spot = 1): every call with the same q (the planner's memo of the
+    gas-stream end point hits) and every call with new q values (every
+    model's Bulirsch-Stoer stream integration runs on the host,
+    crates/roche/src/stream.rs:82-145)."""
+    models = []
+    for text, _ in specs:
+        m = lcb.Model(text=text)
+        m.set_comp("add_spot", "1")
+        models.append(m)
+    q0 = np.array([m.q for m in models])
+    out = {}
+    for case in ("same_q", "new_q"):
+        ms = []
+        for s in range(steps + 1):
+            if case == "new_q":
+                for m, q in zip(models, q0):
+                    m.q = q * (1.0 + 1e-9 * (s + 1))
+            t0 = time.perf_counter()
+            chi, _, _ = lcb.chisq_batch_ragged(models, data, offs, scale=False)
+            if s:
+                ms.append((time.perf_counter() - t0) * 1e3)
+        out[case + "_ms"] = float(np.median(ms))
+    out["stream_ms_per_call"] = out["new_q_ms"] - out["same_q_ms"]
+    out["models"] = len(models)
+    out["failed_models"] = int(np.count_nonzero(~np.isfinite(chi)))
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU path (the oracle, the FP64 restatement of the
     reference's Rayon chisq_batch, built for this host's CPU) on the same
@@ -478,6 +508,12 @@ def main():
         e2e = {"value": weak_value(world, args.models, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "matches_resident": same}
 
+    # ---- bright-spot models: the host's gas-stream integration when q changes every call
+    spot = None
+    if not args.no_e2e and world == 1:
+        spot = {"batch_1024": spot_stream_timing(lcb, specs, pdata, offs),
+                "batch_16": spot_stream_timing(lcb, specs[:16], pdata[:offs[16]], offs[:17])}
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -562,6 +598,7 @@ def main():
                    "parallelism": f"weak, {world} independent batches"},
         "roofline": roof,
         "parity": parity or None,
+        "spot_stream": spot,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": 6 * args.steps,

@@ -151,6 +151,26 @@ int lcb_light_curve_noalloc(lcb_ctx* ctx, const lcb_model* model, const lcb_datu
 int lcb_model_grid(lcb_ctx* ctx, const lcb_model* model, int which, int64_t* n, double* posn, double* dirn,
                    float* area, float* gravity, float* flux, double* ecl);
 
+/* ---- one model split into element slabs (no reference counterpart) --------
+ * The reference builds a model's grids and eclipses serially per star
+ * (crates/lcurve/src/grid.rs:227-320); for a model too large for one device's
+ * time budget the element stage splits into slabs over devices:
+ * lcb_model_elements computes elements [first, first + count) of the model's
+ * element list (grids, continuum and eclipse intervals) into caller-owned
+ * DEVICE arrays of count records each -- rec float4 {dirn, flux}, pos float4
+ * {posn, 0}, p64 double4 {posn, area}, d64 double4 {dirn, gravity}, ecl 4 x
+ * double2 (ingress, egress), unused (+inf, -inf) -- and sets *total to the
+ * model's element count (rec_dev NULL: only *total).  After the slabs are
+ * gathered into full arrays on a device (the order of lcb_model_elements),
+ * lcb_light_curve_elements computes the light curve from them as
+ * lcb_light_curve would, without recomputing any element.  A search that
+ * reaches the eclipse-search bound fails the slab with LCB_ERR_DEVICE_CHECK. */
+int lcb_model_elements(lcb_ctx* ctx, const lcb_model* model, int64_t first, int64_t count, void* rec_dev,
+                       void* pos_dev, void* p64_dev, void* d64_dev, void* ecl_dev, int64_t* total);
+int lcb_light_curve_elements(lcb_ctx* ctx, const lcb_model* model, const lcb_datum* data, int64_t n,
+                             int scale, int rdata, const void* rec_dev, const void* pos_dev, const void* p64_dev,
+                             const void* d64_dev, const void* ecl_dev, double* calc_out, lcb_result* res_out);
+
 /* ---- batched chi-squared ---------------------------------------------------
  * chisq_batch(base, data, names, values, scale) (orchestration.rs:329-357)
  * and chisq_batch_gpu (crates/lcurve-cuda/src/batch.rs:73-80): values is an

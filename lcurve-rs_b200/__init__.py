@@ -181,8 +181,9 @@ class Model:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
-            _capi._lib.lcb_model_destroy(h)
+        lib = getattr(_capi, "_lib", None) if _capi is not None else None  # None at interpreter exit
+        if h and lib is not None:
+            lib.lcb_model_destroy(h)
             self._h = None
 
     # ---- parameters (python/src/lib.rs:263-421)
@@ -353,8 +354,9 @@ class Batch:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
-            _capi._lib.lcb_batch_destroy(h)
+        lib = getattr(_capi, "_lib", None) if _capi is not None else None  # None at interpreter exit
+        if h and lib is not None:
+            lib.lcb_batch_destroy(h)
             self._h = None
 
     def set_params(self, names, values) -> None:

@@ -188,32 +188,45 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     D.firsthit.ensure((P.roche_split > 1 ? P.rblocks.size() * lcb::kRocheBlock : 1) * sizeof(int));
 }
 
-// The device launch sequence of one batch evaluation.
-void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rdata, bool timed) {
+// Parts of the launch sequence: the element stage (grids, continuum, eclipses:
+// k_elements, k_roche) and the rest (k_phase, k_aux, k_flux, k_epilogue).
+constexpr int kStageElements = 1, kStageRest = 2, kStagesAll = 3;
+
+// The device launch sequence of one batch evaluation.  nblk / nrblk (>= 0)
+// launch only the first nblk element blocks and nrblk Roche blocks of the
+// uploaded block lists (an element slab, lcb_model_elements).
+void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rdata, bool timed,
+                 int stages = kStagesAll, int64_t nblk = -1, int64_t nrblk = -1) {
     cudaStream_t s = C->stream;
     const int64_t nm = (int64_t)P.models.size();
+    if (nblk < 0) nblk = (int64_t)P.eblocks.size();
+    if (nrblk < 0) nrblk = (int64_t)P.rblocks.size();
     CUDA_TRY(cudaMemsetAsync(D.aux.p, 0, nm * lcb::kNumAux * sizeof(double), s));
     CUDA_TRY(cudaMemsetAsync(D.status.p, 0, nm * sizeof(int), s));
     CUDA_TRY(cudaMemsetAsync(D.counter.p, 0, sizeof(int) * 4, s));
     CUDA_TRY(cudaMemsetAsync(D.ecount.p, 0, sizeof(unsigned long long) * 8, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[0], s));
+    const bool rest = stages & kStageRest, elem = stages & kStageElements;
     lcb::PhaseArgs pa{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dmodel.as<int32_t>(),
                       D.dsub0.as<int64_t>(), P.ndatum, D.spe.as<float4>(), D.spphi.as<double>(),
                       D.sptype.as<int8_t>(), D.spw.as<double>(), D.slfac.as<double>()};
-    CUDA_TRY(lcb::launch_phase(pa, s));
+    if (rest) CUDA_TRY(lcb::launch_phase(pa, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[1], s));
     lcb::ElemArgs ea{D.models.as<lcb::ModelDev>(), D.segs.as<lcb::SegDesc>(), D.eblocks.as<lcb::ElemBlock>(),
                      D.rblocks.as<lcb::ElemBlock>(), D.ablocks.as<lcb::ElemBlock>(), D.bands.as<lcb::Band>(),
                      D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
                      D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
-                     (int64_t)P.eblocks.size(), (int64_t)P.rblocks.size(), (int64_t)P.ablocks.size(),
+                     nblk, nrblk, (int64_t)P.ablocks.size(),
                      D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>(), C->fblink_cap};
-    if (P.roche_split > 1)
-        CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, P.rblocks.size() * lcb::kRocheBlock * sizeof(int), s));
-    CUDA_TRY(lcb::launch_elements(ea, s));
+    if (elem) {
+        if (P.roche_split > 1 && nrblk > 0)
+            CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, nrblk * lcb::kRocheBlock * sizeof(int), s));
+        CUDA_TRY(lcb::launch_elements(ea, s));
+    }
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[2], s));
-    CUDA_TRY(lcb::launch_roche(ea, s));
+    if (elem) CUDA_TRY(lcb::launch_roche(ea, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[3], s));
+    if (!rest) return;
     CUDA_TRY(lcb::launch_aux(ea, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[4], s));
     lcb::FluxArgs fa{D.models.as<lcb::ModelDev>(), D.units.as<lcb::FluxUnit>(), (int64_t)P.units.size(),
@@ -536,6 +549,93 @@ int lcb_model_grid(lcb_ctx* C, const lcb_model* model, int which, int64_t* n, do
                     ecl[8 * i + 2 * k + 1] = e[i * lcb::kMaxEcl + k].y;
                 }
         }
+    });
+}
+
+// Element records of one model exchanged across devices (a model split into element slabs):
+// five device arrays in the engine's own layout and order.
+struct ElemViews {
+    void* rec; void* pos; void* p64; void* d64; void* ecl;
+};
+static const size_t kElemBytes[5] = {sizeof(float4), sizeof(float4), sizeof(double4), sizeof(double4),
+                                     lcb::kMaxEcl * sizeof(double2)};
+
+int lcb_model_elements(lcb_ctx* C, const lcb_model* model, int64_t first, int64_t count, void* rec_dev,
+                       void* pos_dev, void* p64_dev, void* d64_dev, void* ecl_dev, int64_t* total) {
+    if (!C || !model || !total || first < 0 || count < 0) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] {
+        const lcb::Model* mp = &model->m;
+        lcb_datum d{};
+        d.ferr = 1.0; d.weight = 1.0; d.ndiv = 1;
+        int64_t st = 0, cnt = 1;
+        lcb::Plan& P = C->plan;
+        lcb::plan_batch(&mp, 1, &d, &st, &cnt, C->num_sms, P);
+        if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
+        *total = P.nelem;
+        if (!rec_dev) return;
+        if (!pos_dev || !p64_dev || !d64_dev || !ecl_dev) throw Error(LCB_ERR_INVALID, "null device array");
+        if (first + count > P.nelem) throw Error(LCB_ERR_INVALID, "element range beyond the model's elements");
+        if (count == 0) return;
+        // the element blocks and Roche blocks that touch [first, first + count): every Roche
+        // block lies inside an element block, so the slab's elements are all computed
+        const int64_t last = first + count;
+        auto touches = [&](const lcb::ElemBlock& b, int64_t width) {
+            const int64_t e0 = P.segs[b.seg].first + b.offset;
+            return e0 < last && e0 + width > first;
+        };
+        std::vector<lcb::ElemBlock> eb, rb;
+        for (const auto& b : P.eblocks)
+            if (touches(b, lcb::kElemThreads)) eb.push_back(b);
+        for (const auto& b : P.rblocks)
+            if (touches(b, lcb::kRocheBlock)) rb.push_back(b);
+        upload_plan(C, C->scratch, P, &d, 1, true);
+        DeviceSet& D = C->scratch;
+        if (!eb.empty())
+            CUDA_TRY(cudaMemcpyAsync(D.eblocks.p, eb.data(), eb.size() * sizeof(lcb::ElemBlock),
+                                     cudaMemcpyHostToDevice, C->stream));
+        if (!rb.empty())
+            CUDA_TRY(cudaMemcpyAsync(D.rblocks.p, rb.data(), rb.size() * sizeof(lcb::ElemBlock),
+                                     cudaMemcpyHostToDevice, C->stream));
+        enqueue_run(C, D, P, 0, 0, false, kStageElements, (int64_t)eb.size(), (int64_t)rb.size());
+        void* dst[5] = {rec_dev, pos_dev, p64_dev, d64_dev, ecl_dev};
+        const void* src[5] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p, D.ecl.p};
+        for (int k = 0; k < 5; ++k)
+            CUDA_TRY(cudaMemcpyAsync(dst[k], (const char*)src[k] + first * kElemBytes[k], count * kElemBytes[k],
+                                     cudaMemcpyDeviceToDevice, C->stream));
+        int status = 0;
+        CUDA_TRY(cudaMemcpyAsync(&status, D.status.p, sizeof(int), cudaMemcpyDeviceToHost, C->stream));
+        CUDA_TRY(cudaStreamSynchronize(C->stream));
+        if (status & lcb::kStatusIterCap)
+            throw Error(LCB_ERR_DEVICE_CHECK, "a device-side iteration cap tripped for this model");
+    });
+}
+
+int lcb_light_curve_elements(lcb_ctx* C, const lcb_model* model, const lcb_datum* data, int64_t n, int scale,
+                             int rdata, const void* rec_dev, const void* pos_dev, const void* p64_dev,
+                             const void* d64_dev, const void* ecl_dev, double* calc_out, lcb_result* res_out) {
+    if (!C || !model || (!data && n > 0) || !calc_out || !rec_dev || !pos_dev || !p64_dev || !d64_dev || !ecl_dev)
+        return fail(LCB_ERR_INVALID, "null pointer");
+    if (n <= 0) return fail(LCB_ERR_EMPTY, "No data points");
+    return guarded(C, [&] {
+        const lcb::Model* mp = &model->m;
+        int64_t st = 0, cnt = n;
+        lcb::Plan& P = C->plan;
+        lcb::plan_batch(&mp, 1, data, &st, &cnt, C->num_sms, P);
+        if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
+        upload_plan(C, C->scratch, P, data, 0, true);
+        DeviceSet& D = C->scratch;
+        const void* src[5] = {rec_dev, pos_dev, p64_dev, d64_dev, ecl_dev};
+        void* dst[5] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p, D.ecl.p};
+        for (int k = 0; k < 5; ++k)
+            if (P.nelem)
+                CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], P.nelem * kElemBytes[k], cudaMemcpyDeviceToDevice, C->stream));
+        enqueue_run(C, D, P, scale, rdata, false, kStageRest);
+        std::vector<double> res, calc;
+        std::vector<int> status;
+        fetch_results(C, D, P, res, &calc, &status);
+        if (status[0] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+        std::memcpy(calc_out, calc.data(), n * sizeof(double));
+        if (res_out) fill_result(res.data(), res_out);
     });
 }
 

@@ -1,4 +1,10 @@
-"""One model's light curve split across GPUs by time (one process per GPU).
+"""Work split across GPUs, one process per GPU (torch.distributed).
+
+chisq_batch_sharded: one batch of models divided among the ranks by a cost
+estimate (the reference's chisq_batch model loop, orchestration.rs:343-356),
+each rank evaluating its models in one batch, the chi-squared all-gathered.
+
+light_curve_sharded: one model's light curve split across GPUs by time.
 
 The data (times) of a single large model are divided into contiguous shards,
 one per rank of a torch.distributed process group (`mcmc.shard_bounds`).
@@ -180,3 +186,105 @@ def chisq_batch_sharded(models, data: np.ndarray, offsets, scale: bool = False, 
     for r in range(world):
         out[parts[r]] = got[r][:parts[r].size].cpu().numpy()
     return out
+
+
+# ---------------------------------------------------------------------------
+# One model's element stage split into slabs across GPUs, then its flux sum
+# split by time (the grids and eclipse intervals of a ~5 M-element model are
+# per-element work: crates/lcurve/src/grid.rs:227-320)
+# ---------------------------------------------------------------------------
+ELEMENT_ARRAYS = ("rec", "pos", "p64", "d64", "ecl")
+ELEMENT_BYTES = (16, 16, 32, 32, 64)   # per element: float4, float4, double4, double4, 4 x double2
+
+
+class EngineElements:
+    """The GPU engine as an element source: slabs by lcb_model_elements into
+    device tensors (uint8 rows of the records' bytes), light curves from a
+    full element set by lcb_light_curve_elements."""
+
+    def __init__(self, model):
+        from . import _capi, _ctx  # noqa: PLC0415
+        self.model, self._capi, self._ctx = model, _capi, _ctx
+        self.L = _capi.load()
+
+    def total(self) -> int:
+        import ctypes as C  # noqa: PLC0415
+        n = C.c_int64()
+        self._capi.check(self.L.lcb_model_elements(self._ctx(), self.model._h, 0, 0, None, None, None, None, None,
+                                                   C.byref(n)))
+        return n.value
+
+    def slab(self, first: int, count: int):
+        import ctypes as C  # noqa: PLC0415
+        import torch  # noqa: PLC0415
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = [torch.empty((max(count, 1), b), dtype=torch.uint8, device=dev) for b in ELEMENT_BYTES]
+        torch.cuda.synchronize()
+        n = C.c_int64()
+        if count:
+            self._capi.check(self.L.lcb_model_elements(self._ctx(), self.model._h, first, count,
+                                                       *[C.c_void_p(t.data_ptr()) for t in out], C.byref(n)))
+        return [t[:count] for t in out]
+
+    def evaluate(self, arrays, shard: np.ndarray):
+        import ctypes as C  # noqa: PLC0415
+        import torch  # noqa: PLC0415
+        from . import Result, dptr  # noqa: PLC0415
+        shard = np.ascontiguousarray(shard, dtype=DATUM_DTYPE)
+        arrays = [a.contiguous() for a in arrays]
+        torch.cuda.synchronize()
+        calc = np.zeros(shard.shape[0])
+        res = Result()
+        self._capi.check(self.L.lcb_light_curve_elements(self._ctx(), self.model._h, shard.ctypes.data,
+                                                         shard.shape[0], 0, 1,
+                                                         *[C.c_void_p(a.data_ptr()) for a in arrays],
+                                                         dptr(calc), C.byref(res)))
+        return calc, dict(wdwarf=res.wdwarf, logg1=res.logg1, logg2=res.logg2, rv1=res.rv1, rv2=res.rv2)
+
+
+def _gather_records(local, counts, group):
+    """All ranks' record slabs (per array: a (count, bytes) uint8 tensor) in
+    rank order, concatenated; each array is sent padded to the largest slab."""
+    import torch  # noqa: PLC0415
+    import torch.distributed as dist  # noqa: PLC0415
+    world = dist.get_world_size(group)
+    width = max(max(counts), 1)
+    out = []
+    for a in local:
+        buf = torch.zeros((width, a.shape[1]), dtype=torch.uint8, device=a.device)
+        buf[:a.shape[0]] = a
+        parts = [torch.empty_like(buf) for _ in range(world)]
+        dist.all_gather(parts, buf, group=group)
+        out.append(torch.cat([parts[r][:counts[r]] for r in range(world)]))
+    return out
+
+
+def light_curve_element_split(model, data: np.ndarray, scale: bool = False, group=None, source=None) -> LcResult:
+    """Light curve of one large model with both stages divided among the ranks
+    of `group` (every rank passes the same model and data): the element list
+    is cut into equal contiguous slabs (mcmc.shard_bounds), each rank computes
+    its slab's grid points, continuum and eclipse intervals, the slabs are
+    all-gathered into the full element set on every rank (each rank's own
+    device memory; 160 B an element), and then the flux sum is split by time
+    as light_curve_sharded does, every rank evaluating its share of the data
+    from the gathered elements.  Returns what Model.light_curve(data=data,
+    scale=scale) returns.
+
+    source: the element source (total(), slab(first, count) -> per-array
+    (count, bytes) uint8 tensors, evaluate(arrays, shard) -> (unscaled
+    fluxes, {wdwarf, logg1, logg2, rv1, rv2})); by default the GPU engine."""
+    if source is None:
+        if model.get_comp("iscale") not in ("0", "false"):
+            raise ValueError("per-component scaling (iscale = 1) is not split across ranks")
+        source = EngineElements(model)
+    total = source.total()
+    if group is None:
+        arrays = source.slab(0, total)
+    else:
+        import torch.distributed as dist  # noqa: PLC0415
+        b = shard_bounds(total, dist.get_world_size(group))
+        r = dist.get_rank(group)
+        counts = [b[k + 1] - b[k] for k in range(len(b) - 1)]
+        arrays = _gather_records(source.slab(b[r], counts[r]), counts, group)
+    return light_curve_sharded(model, data, scale=scale, group=group,
+                               evaluate=lambda m, shard: source.evaluate(arrays, shard))

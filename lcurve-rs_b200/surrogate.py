@@ -194,8 +194,9 @@ class Surrogate:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _capi._lib is not None:
-            _capi._lib.lcb_mlp_destroy(h)
+        lib = getattr(_capi, "_lib", None) if _capi is not None else None  # None at interpreter exit
+        if h and lib is not None:
+            lib.lcb_mlp_destroy(h)
             self._h = None
 
     def _x(self, theta):

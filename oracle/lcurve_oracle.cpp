@@ -2512,6 +2512,22 @@ int orc_grids_fetch(void* gh, int which, double* posn, double* dirn, float* area
     }
     return 0;
 }
+// Replaces the points of one grid (same arrays as orc_grids_fetch), for light curves on
+// element sets assembled elsewhere (the slab-split tests).
+int orc_grids_set(void* gh, int which, int64_t n, const double* posn, const double* dirn, const float* area,
+                  const float* gravity, const float* flux, const int* necl, const double* ecl) {
+    Pts* p = const_cast<Pts*>(grid_sel((OrcGrids*)gh, which));
+    if (!p) return 1;
+    p->assign((size_t)n, Point());
+    for (int64_t i = 0; i < n; ++i) {
+        Point& pt = (*p)[i];
+        pt.posn = Vec3(posn[3 * i], posn[3 * i + 1], posn[3 * i + 2]);
+        pt.dirn = Vec3(dirn[3 * i], dirn[3 * i + 1], dirn[3 * i + 2]);
+        pt.area = area[i]; pt.gravity = gravity[i]; pt.flux = flux[i];
+        for (int k = 0; k < necl[i] && k < 4; ++k) pt.eclipse.push_back({ecl[8 * i + 2 * k], ecl[8 * i + 2 * k + 1]});
+    }
+    return 0;
+}
 // gint scales, rlens1, bright-spot position: 10 doubles
 void orc_grids_info(void* gh, double* out) {
     Grids& g = ((OrcGrids*)gh)->g;

@@ -57,8 +57,8 @@ def use_native() -> str:
         pass
     key = hashlib.sha1((host_cpu() + flags).encode()).hexdigest()[:12]
     so = HERE / "_native" / f"liblcurve_oracle_{key}.so"
-    if not so.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_SO=_native/{so.name}"], check=True)
+    # make rebuilds it when the source is newer
+    subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_SO=_native/{so.name}"], check=True)
     LIB_PATH = so
     return str(so)
 
@@ -92,6 +92,8 @@ def lib():
     L.orc_grids_info.argtypes = [vp, dp]
     L.orc_grids_light_curve.argtypes = [vp, vp, vp, ip, ip, ip, ip, dp, dp, cp, ip]
     L.orc_set_grid_threads.argtypes = [ip]
+    L.orc_grids_set.argtypes = [vp, ip, C.c_int64, dp, dp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                C.POINTER(C.c_float), C.POINTER(C.c_int), dp]
     for f in ("orc_xl1",):
         getattr(L, f).argtypes = [C.c_double]
         getattr(L, f).restype = C.c_double
@@ -253,6 +255,19 @@ class Grids:
                               flux.ctypes.data_as(C.POINTER(C.c_float)),
                               necl.ctypes.data_as(C.POINTER(C.c_int)), _dp(ecl))
         return dict(posn=posn, dirn=dirn, area=area, gravity=grav, flux=flux, necl=necl, ecl=ecl)
+
+    def store(self, name: str, g: dict) -> None:
+        """Replaces grid `name` with the arrays of `g` (the layout fetch returns)."""
+        n = g["posn"].shape[0]
+        fp = C.POINTER(C.c_float)
+        arr = {k: np.ascontiguousarray(g[k]) for k in ("posn", "dirn", "ecl")}
+        f32 = {k: np.ascontiguousarray(g[k], dtype=np.float32) for k in ("area", "gravity", "flux")}
+        necl = np.ascontiguousarray(g["necl"], dtype=np.int32)
+        if lib().orc_grids_set(self._g, GRID_NAMES[name], n, _dp(arr["posn"]), _dp(arr["dirn"]),
+                               f32["area"].ctypes.data_as(fp), f32["gravity"].ctypes.data_as(fp),
+                               f32["flux"].ctypes.data_as(fp), necl.ctypes.data_as(C.POINTER(C.c_int)),
+                               _dp(arr["ecl"])) != 0:
+            raise OracleError("bad grid name")
 
     def info(self):
         info = np.zeros(10)

@@ -31,6 +31,8 @@ def _models(lcb):
     roche = lcb.Model(GOLDEN / "test_model.dat")  # star 2 fills its Roche lobe: star 1 needs the Roche search
     sphere = roche.copy()
     sphere.set_comp("roche2", "0")  # both stars spheres: analytic eclipses only, the cap never applies
+    for k in ("nlat1c", "nlat2c"):    # one grid per star (no ginterp ratio, which is 0/0 when the
+        sphere.set_comp(k, sphere.get_comp(k.replace("c", "f")))  # larger sphere hides star 1 at phase1)
     return roche, sphere
 
 

@@ -256,3 +256,75 @@ def test_batch_tuning_keeps_results(lcb, W):
             assert np.allclose(chi, chi0, rtol=1e-4, atol=0), tune
     B.set_tuning(0, 0, 0)
     assert B.tuning() == heuristic
+
+
+def test_batch_split_through_nccl_matches_the_unsplit_batch(lcb, W):
+    """sharded.chisq_batch_sharded (models weighed by lcb_model_work, split by
+    cost, chi-squared all-gathered) through a one-rank NCCL group, with device
+    tensors in the all-gather: the same chi-squared as chisq_batch_ragged."""
+    import importlib
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    S = importlib.import_module("lcurve-rs_b200.sharded")
+    specs = W.batch_models(n=9, seed=13, nlat1=(20, 40), nlat2=(30, 60), ntime=(100, 250))
+    models = [lcb.Model(text=s) for s, _ in specs]
+    offs = np.zeros(len(specs) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(t) for _, t in specs])
+    t = np.concatenate([t for _, t in specs])
+    data = lcb.make_data(t, expose=0.001, ndiv=1, ferr=0.001, weight=1.0)
+    data["flux"] = 0.02 + 0.004 * np.cos(2 * np.pi * t)
+    ref, _, _ = lcb.chisq_batch_ragged(models, data, offs, scale=True)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        got = S.chisq_batch_sharded(models, data, offs, scale=True, group=dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+    assert np.all(np.isfinite(ref)) and np.allclose(got, ref, rtol=1e-12, atol=0)
+    assert np.allclose(S.chisq_batch_sharded(models, data, offs, scale=True), ref, rtol=1e-12, atol=0)
+
+
+def test_element_slabs_match_light_curve(lcb, W):
+    """lcb_model_elements in two slabs, concatenated on the device, then
+    lcb_light_curve_elements: lcb_light_curve's fluxes (the records are per
+    element, the flux plan is the same); and sharded.light_curve_element_split
+    through a one-rank NCCL group: Model.light_curve(scale=True)."""
+    import importlib
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    S = importlib.import_module("lcurve-rs_b200.sharded")
+    text, t, expose, ndiv = W.single_large(nlat1=60, nlat2=120, ntime=600, nrad=60, nspot=40)
+    m = lcb.Model(text=text)
+    d = lcb.make_data(t, expose=expose, ndiv=ndiv, ferr=0.01, weight=1.0)
+    d["flux"] = 0.02 + 0.004 * np.cos(2 * np.pi * t)
+    ref = m.light_curve(data=d, scale=False)
+    src = S.EngineElements(m)
+    total = src.total()
+    k = total // 3
+    full = [torch.cat([x, y]) for x, y in zip(src.slab(0, k), src.slab(k, total - k))]
+    calc, per = src.evaluate(full, d)
+    assert np.allclose(calc, ref.calc, rtol=1e-12, atol=0)
+    assert per["wdwarf"] == pytest.approx(ref.wdwarf, rel=1e-12)
+    ref_s = m.light_curve(data=d, scale=True)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=120), device_id=torch.device("cuda", 0))
+    try:
+        r = S.light_curve_element_split(m, d, scale=True, group=dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+    assert np.allclose(r.calc, ref_s.calc, rtol=1e-12, atol=0)
+    assert r.chisq == pytest.approx(ref_s.chisq, rel=1e-12) and r.wnok == ref_s.wnok

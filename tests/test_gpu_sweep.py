@@ -6,7 +6,8 @@ spots, edge cases), each light curve at 50 times in [-0.2, 1.2] on the GPU
 against the oracle.  The reference's threshold there is max relative error
 1e-5 (run_regression100.py:33), the same as here.  Where the oracle's light
 curve is NaN (a ginterp ratio of two zero sums when the primary is eclipsed at
-phase1, orchestration.rs:93-131) the GPU's must be NaN at the same points.
+phase1, orchestration.rs:93-131) the GPU's must be NaN at the same points,
+and where it is exactly 0 (t2 < 0 with the primary eclipsed) so must the GPU's.
 """
 import importlib
 import os
@@ -35,7 +36,9 @@ def test_model_sweep_vs_oracle(lcb, oracle):
     for (kind, text), o in zip(sweep, refs):
         g = lcb.Model(text=text).light_curve(times=t, expose=0.001, ndiv=1).flux
         assert np.array_equal(np.isnan(g), np.isnan(o)), kind
-        ok = np.isfinite(o)
+        # exact zeros (both stars dark or hidden: t2 < 0 and the primary eclipsed) must be zeros
+        assert np.array_equal(g[o == 0.0], o[o == 0.0]), kind
+        ok = np.isfinite(o) & (o != 0.0)
         if ok.any():
             err = float(np.max(np.abs(g[ok] - o[ok]) / np.abs(o[ok])))
             worst[kind] = max(worst.get(kind, 0.0), err)
