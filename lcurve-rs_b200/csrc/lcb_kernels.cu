@@ -12,7 +12,7 @@
 //                star keep that slot for k_roche.
 //   k_roche    : one thread per element eclipsed by a Roche-distorted star:
 //                the FP64 ray-march ingress_egress (eclipse.rs:270-373), the
-//                phase scan with exact lower-bound miss proofs, then the two
+//                phase scan with exact second-order miss proofs, then the two
 //                bisections.  Small batches run k_roche_scan (the scan split
 //                over several threads, first hit by atomicMin) and
 //                k_roche_chop2 (the ingress and egress bisections from that
@@ -54,10 +54,10 @@ constexpr double kEfac = 1.0000001;                               // grid.rs:396
 #define LCB_ROCHE_MIN_BLOCKS 5
 #endif
 #ifndef LCB_CERT_BUDGET
-#define LCB_CERT_BUDGET 24
+#define LCB_CERT_BUDGET 32
 #endif
 constexpr int kRocheMinBlocks = LCB_ROCHE_MIN_BLOCKS;  // k_roche blocks per SM (128 threads): register budget
-constexpr int kCertBudget = LCB_CERT_BUDGET;           // lower-bound nodes per line of sight before the full search
+constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per line of sight before the full search
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 __device__ __forceinline__ double rad2deg(double r) { return r * (180.0 / kPi); }
@@ -200,48 +200,61 @@ __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double 
     return false;  // iteration cap: the reference maps its Err to "not eclipsed"
 }
 
-// Rigorous lower bound of the Roche potential on the segment p + lam*e,
-// lam in [a, b] (|e| = 1): the two gravity terms are bounded at the closest
-// approach to each star, the centrifugal term (convex along a line) and the
-// linear term at the end points.
-__device__ __forceinline__ double pot_lower_bound(const RocheEcl& s, const Los& L, double a, double b) {
-    // distance to the primary (origin)
+// Squared distances from the segment p + lam*e, lam in [a, b] (|e| = 1), to the
+// two stars' centres (the primary at the origin, the secondary at (1, 0, 0)).
+__device__ __forceinline__ void closest_sq(const Los& L, double a, double b, double& d1, double& d2) {
     double t1 = fmin(fmax(-(L.px * L.ex + L.py * L.ey + L.pz * L.ez), a), b);
     double x1 = fma(t1, L.ex, L.px), y1 = fma(t1, L.ey, L.py), z1 = fma(t1, L.ez, L.pz);
-    double d1 = x1 * x1 + y1 * y1 + z1 * z1;
-    // distance to the secondary (1, 0, 0)
+    d1 = x1 * x1 + y1 * y1 + z1 * z1;
     double qx = L.px - 1.0;
     double t2 = fmin(fmax(-(qx * L.ex + L.py * L.ey + L.pz * L.ez), a), b);
     double x2 = fma(t2, L.ex, qx), y2 = fma(t2, L.ey, L.py), z2 = fma(t2, L.ez, L.pz);
-    double d2 = x2 * x2 + y2 * y2 + z2 * z2;
-    double xa = fma(a, L.ex, L.px), ya = fma(a, L.ey, L.py);
-    double xb = fma(b, L.ex, L.px), yb = fma(b, L.ey, L.py);
-    double lb = -s.comp * rsqrt(d1) - s.mu * rsqrt(d2);
-    // the rest is a concave quadratic along the line: its minimum is at an end point
-    if (s.primary) {  // rpot1: - ssq (x^2+y^2)/2 + mu x
-        double ca = -0.5 * s.ssq * (xa * xa + ya * ya) + s.mu * xa;
-        double cb = -0.5 * s.ssq * (xb * xb + yb * yb) + s.mu * xb;
-        return lb + fmin(ca, cb);
-    }
-    // rpot2: - ssq ((x-1)^2 + y^2)/2 - comp x
-    double ca = -0.5 * s.ssq * ((xa - 1.0) * (xa - 1.0) + ya * ya) - s.comp * xa;
-    double cb = -0.5 * s.ssq * ((xb - 1.0) * (xb - 1.0) + yb * yb) - s.comp * xb;
-    return lb + fmin(ca, cb);
+    d2 = x2 * x2 + y2 * y2 + z2 * z2;
+}
+
+// The potential and its derivative along the line of sight at one point
+// (los_pot and los_dpot sharing the two distances).
+__device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, double lam, double& f, double& df) {
+    double x = fma(lam, L.ex, L.px), y = fma(lam, L.ey, L.py), z = fma(lam, L.ez, L.pz);
+    double x2y2 = x * x + y * y;
+    double r1sq = x2y2 + z * z, r2sq = r1sq + 1.0 - 2.0 * x;
+    double i1 = rsqrt(r1sq), i2 = rsqrt(r2sq);
+    double v = -s.comp * i1 - s.mu * i2;
+    f = s.primary ? v - s.ssq * x2y2 * 0.5 + s.mu * x : v - s.ssq * (0.5 + 0.5 * x2y2 - x) - s.comp * x;
+    double comp = s.comp * (i1 * i1 * i1), mu1 = s.mu * (i2 * i2 * i2);
+    double gx = comp * x + mu1 * (x - 1.0) - (s.primary ? s.ssq * x - s.mu : s.ssq * (x - 1.0) - s.mu + 1.0);
+    double gy = comp * y + mu1 * y - s.ssq * y;
+    double gz = comp * z + mu1 * z;
+    df = gx * L.ex + gy * L.ey + gz * L.ez;
 }
 
 // True when the potential provably stays above the surface value on the whole
 // line-of-sight segment [a, b]: an adaptive march over sub-segments, each
-// certified by pot_lower_bound with a margin of 1e-9 relative (far above the
-// rounding of any potential evaluation).  False means "not proven".
+// certified by a second-order bound.  Along a line the Roche potential's
+// second derivative is at least -M, M = 2 comp / r1^3 + 2 mu / r2^3 + ssq with
+// r1, r2 the segment's closest approaches to the two centres (each gravity
+// term -c / r has second derivative c (r^2 - 3 s^2) / r^5 >= -2 c / r^3, s the
+// distance along the line from the closest point; the centrifugal term
+// -ssq (x^2 + y^2) / 2 contributes -ssq (ex^2 + ey^2) >= -ssq; the rest is
+// linear), so on a sub-segment of length h around m
+//   phi >= phi(m) - |phi'(m)| h / 2 - M h^2 / 8.
+// The bound must clear the surface value by 1e-9 relative (far above the
+// rounding of any evaluation).  False means "not proven".
 __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int& nodes) {
     const double thr = s.pref + 1e-9 * fmax(fabs(s.pref), 1.0);
     const double hmin = 1e-6 * (b - a);
+    double d1, d2;
+    closest_sq(L, a, b, d1, d2);
+    const double i1 = rsqrt(d1), i2 = rsqrt(d2);
+    const double curv = 2.0 * s.comp * (i1 * i1 * i1) + 2.0 * s.mu * (i2 * i2 * i2) + s.ssq;
     double t = a, h = b - a;
     for (int it = 0; it < kCertBudget; ++it) {
         if (t >= b) return true;
         double hh = fmin(h, b - t);
         ++nodes;
-        if (pot_lower_bound(s, L, t, t + hh) > thr) {
+        double f, df;
+        los_pot_dpot(s, L, t + 0.5 * hh, f, df);
+        if (f - fabs(df) * (0.5 * hh) - curv * (0.125 * hh * hh) > thr) {
             t += hh;
             h = 2.0 * hh;
         } else {
@@ -254,7 +267,7 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
 
 // Is point p hidden from earth direction e by the Roche star? (eclipse.rs:123-197)
 // With `prove` set, a line of sight whose first reference evaluation is not
-// inside the star is first tested with the rigorous lower bound: every point
+// inside the star is first tested with the rigorous second-order bound: every point
 // the reference search evaluates lies in [lam1 - acc, lam2 + acc] (dbrent.rs:116
 // may step acc past an end), so a proven miss is exactly its "false".
 // Not inlined: as a call, the search's working set does not add to the
