@@ -6,12 +6,15 @@ the build command when it is missing.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import pathlib
 
 import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
-LIB_PATH = HERE / "liblcurve_b200.so"
+# LCB_LIBRARY selects another build of the library, e.g. the index-checking
+# liblcurve_b200_bounds.so of `make bounds`
+LIB_PATH = pathlib.Path(os.environ["LCB_LIBRARY"]) if os.environ.get("LCB_LIBRARY") else HERE / "liblcurve_b200.so"
 
 LCB_OK = 0
 ERR_NAMES = {

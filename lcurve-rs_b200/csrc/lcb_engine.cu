@@ -207,6 +207,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     CUDA_TRY(cudaMemsetAsync(D.ecount.p, 0, sizeof(unsigned long long) * 8, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[0], s));
     const bool rest = stages & kStageRest, elem = stages & kStageElements;
+    const lcb::Sizes sz{P.nelem, P.nsub, P.npartial, P.ndatum, (int64_t)P.bands.size(), (int64_t)P.rings.size()};
     lcb::PhaseArgs pa{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dmodel.as<int32_t>(),
                       D.dsub0.as<int64_t>(), P.ndatum, D.spe.as<float4>(), D.spphi.as<double>(),
                       D.sptype.as<int8_t>(), D.spw.as<double>(), D.slfac.as<double>()};
@@ -217,7 +218,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
                      D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
                      D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
                      nblk, nrblk, (int64_t)P.ablocks.size(),
-                     D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>(), C->fblink_cap};
+                     D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>(), C->fblink_cap, sz};
     if (elem) {
         if (P.roche_split > 1 && nrblk > 0)
             CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, nrblk * lcb::kRocheBlock * sizeof(int), s));
@@ -232,7 +233,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     lcb::FluxArgs fa{D.models.as<lcb::ModelDev>(), D.units.as<lcb::FluxUnit>(), (int64_t)P.units.size(),
                      D.counter.as<int>(), D.rec.as<float4>(), D.pos.as<float4>(), D.ecl.as<double2>(),
                      D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
-                     D.status.as<int>()};
+                     D.status.as<int>(), sz};
     const int bps_max = lcb::flux_blocks_per_sm();
     const int bps = P.flux_blocks_per_sm > 0 ? std::min(P.flux_blocks_per_sm, bps_max) : bps_max;
     int64_t grid = (int64_t)C->num_sms * bps;
@@ -242,7 +243,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     lcb::EpiArgs pe{D.models.as<lcb::ModelDev>(), D.datum.as<lcb_datum>(), D.dsub0.as<int64_t>(),
                     D.spphi.as<double>(), D.spw.as<double>(), D.slfac.as<double>(), D.partial.as<double>(),
                     D.aux.as<double>(), D.status.as<int>(), scale, rdata, D.calc.as<double>(),
-                    D.results.as<double>(), D.fcomp.as<double>(), D.svda.as<double>(), nm};
+                    D.results.as<double>(), D.fcomp.as<double>(), D.svda.as<double>(), nm, sz, D.status.as<int>()};
     CUDA_TRY(lcb::launch_epilogue(pe, s));
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[6], s));
 }
@@ -266,6 +267,13 @@ void fetch_results(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, std::vector<dou
     C->d2h += (int64_t)(nm * 12 * sizeof(double)) + (calc ? P.ndatum * (int64_t)sizeof(double) : 0) +
               (status ? nm * (int64_t)sizeof(int) : 0);
     CUDA_TRY(cudaStreamSynchronize(C->stream));
+}
+
+// Device checks that fail a whole call (as opposed to one model's NaN): a bounded
+// wait that gave up, or (LCURVE_DEBUG_BOUNDS build) an index out of range.
+void check_device_status(int st) {
+    if (st & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+    if (st & lcb::kStatusBounds) throw Error(LCB_ERR_DEVICE_CHECK, "a device-side bounds check failed");
 }
 
 void fill_result(const double* r, lcb_result* out) {
@@ -296,7 +304,7 @@ void run_transient(lcb_ctx* C, const lcb::Model* const* models, int64_t n, const
         fetch_results(C, C->scratch, P, res, calc, &st);
     }
     for (int64_t i = 0; i < n; ++i)
-        if (st[i] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+        check_device_status(st[i]);
 }
 
 template <class F>
@@ -605,6 +613,7 @@ int lcb_model_elements(lcb_ctx* C, const lcb_model* model, int64_t first, int64_
         int status = 0;
         CUDA_TRY(cudaMemcpyAsync(&status, D.status.p, sizeof(int), cudaMemcpyDeviceToHost, C->stream));
         CUDA_TRY(cudaStreamSynchronize(C->stream));
+        check_device_status(status);
         if (status & lcb::kStatusIterCap)
             throw Error(LCB_ERR_DEVICE_CHECK, "a device-side iteration cap tripped for this model");
     });
@@ -633,7 +642,7 @@ int lcb_light_curve_elements(lcb_ctx* C, const lcb_model* model, const lcb_datum
         std::vector<double> res, calc;
         std::vector<int> status;
         fetch_results(C, D, P, res, &calc, &status);
-        if (status[0] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+        check_device_status(status[0]);
         std::memcpy(calc_out, calc.data(), n * sizeof(double));
         if (res_out) fill_result(res.data(), res_out);
     });
@@ -858,7 +867,7 @@ int lcb_batch_run(lcb_batch* B, int scale) {
         CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
         B->ran = true;
         for (int s : B->h_status)
-            if (s & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+            check_device_status(s);
     });
 }
 
@@ -877,7 +886,7 @@ int lcb_batch_profile(lcb_batch* B, int scale) {
         }
         B->ran = true;
         for (int s : B->h_status)
-            if (s & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+            check_device_status(s);
     });
 }
 
@@ -1120,7 +1129,7 @@ extern "C" int lcb_light_curve_noalloc(lcb_ctx* C, const lcb_model* model, const
             cudaStreamSynchronize(C->stream);  // no work may touch the arena after the lock is released
             throw;
         }
-        if (status[0] & lcb::kStatusTmaTimeout) throw Error(LCB_ERR_DEVICE_CHECK, "a bounded device wait timed out");
+        check_device_status(status[0]);
         if (status[0] & lcb::kStatusIterCap)
             throw Error(LCB_ERR_DEVICE_CHECK, "a device-side iteration cap tripped for this model");
         std::memcpy(calc_out, calc.data(), n * sizeof(double));

@@ -173,5 +173,6 @@ constexpr int kFblinkEvalCap = 1 << 18;
 // Device status bits (ModelDev.status / batch status word).
 constexpr int kStatusIterCap = 1;     // an iteration cap without a reference counterpart tripped
 constexpr int kStatusTmaTimeout = 2;  // a bounded mbarrier wait gave up
+constexpr int kStatusBounds = 4;      // LCURVE_DEBUG_BOUNDS build: an index check failed (access skipped)
 
 }  // namespace lcb

@@ -44,6 +44,15 @@ namespace lcb {
 
 namespace {
 
+// LCURVE_DEBUG_BOUNDS build (make bounds): index checks that record
+// kStatusBounds for the model and skip the access instead of reading or
+// writing out of range; in the normal build they compile to nothing.
+#ifdef LCURVE_DEBUG_BOUNDS
+#define LCB_IN_BOUNDS(cond, status_word) ((cond) || (atomicOr((status_word), kStatusBounds), false))
+#else
+#define LCB_IN_BOUNDS(cond, status_word) true
+#endif
+
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr double kFac1 = 2.0e27 * 6.6262e-34 * 2.99792458e8;      // planck.rs:5
@@ -58,6 +67,10 @@ constexpr double kEfac = 1.0000001;                               // grid.rs:396
 #endif
 constexpr int kRocheMinBlocks = LCB_ROCHE_MIN_BLOCKS;  // k_roche blocks per SM (128 threads): register budget
 constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per line of sight before the full search
+#ifndef LCB_CHOP_BUDGET
+#define LCB_CHOP_BUDGET 0
+#endif
+constexpr int kChopBudget = LCB_CHOP_BUDGET;           // the same in the bisections (0: no proofs there)
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 __device__ __forceinline__ double rad2deg(double r) { return r * (180.0 / kPi); }
@@ -240,7 +253,7 @@ __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, do
 //   phi >= phi(m) - |phi'(m)| h / 2 - M h^2 / 8.
 // The bound must clear the surface value by 1e-9 relative (far above the
 // rounding of any evaluation).  False means "not proven".
-__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int& nodes) {
+__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int budget, int& nodes) {
     const double thr = s.pref + 1e-9 * fmax(fabs(s.pref), 1.0);
     const double hmin = 1e-6 * (b - a);
     double d1, d2;
@@ -248,7 +261,7 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
     const double i1 = rsqrt(d1), i2 = rsqrt(d2);
     const double curv = 2.0 * s.comp * (i1 * i1 * i1) + 2.0 * s.mu * (i2 * i2 * i2) + s.ssq;
     double t = a, h = b - a;
-    for (int it = 0; it < kCertBudget; ++it) {
+    for (int it = 0; it < budget; ++it) {
         if (t >= b) return true;
         double hh = fmin(h, b - t);
         ++nodes;
@@ -266,14 +279,14 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
 }
 
 // Is point p hidden from earth direction e by the Roche star? (eclipse.rs:123-197)
-// With `prove` set, a line of sight whose first reference evaluation is not
+// With `prove` > 0 (a node budget), a line of sight whose first reference evaluation is not
 // inside the star is first tested with the rigorous second-order bound: every point
 // the reference search evaluates lies in [lam1 - acc, lam2 + acc] (dbrent.rs:116
 // may step acc past an end), so a proven miss is exactly its "false".
 // Not inlined: as a call, the search's working set does not add to the
 // registers the surrounding scan/bisection loop keeps live, which lets the
 // kernel run 5 blocks per SM (451 -> 350 ms on the 1024-model batch).
-__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, bool prove) {
+__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, int prove) {
     ++cnt.fbl;
     double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
     double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
@@ -292,9 +305,9 @@ __device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L,
     double flam = los_pot(s, L, lam0);
     ++cnt.pot;
     if (flam <= pref) return true;
-    if (prove) {
+    if (prove > 0) {  // prove: the miss-proof node budget (0: no proof)
         const double pad = 1.001 * acc + 1e-12;
-        if (certify_miss(s, L, lam1 - pad, lam2 + pad, cnt.cert)) { ++cnt.skipped; return false; }
+        if (certify_miss(s, L, lam1 - pad, lam2 + pad, prove, cnt.cert)) { ++cnt.skipped; return false; }
     }
     int nstep = 1;
     double f1 = los_pot(s, L, lam1), f2 = los_pot(s, L, lam2), lam = lam0;
@@ -427,7 +440,7 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
             ph = (pin + pout) / 2.0;
         }
         earth_at(cosi, sini, ph, L.ex, L.ey, L.ez);
-        const bool hit = fblink(s, acc, L, evals, capped, mode == SCAN && kCertBudget > 0);
+        const bool hit = fblink(s, acc, L, evals, capped, mode == SCAN ? kCertBudget : kChopBudget);
         if (capped) return false;
         if (mode == SCAN) {
             if (hit) { phi = ph; mode = CHOP_IN; pin = phi; pout = phi1; it = 0; }
@@ -630,6 +643,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
             int mid = (lo + hi + 1) >> 1;
             if (A.bands[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
         }
+        if (!LCB_IN_BOUNDS(sg.table + lo < A.sz.nbands && sg.first + i < A.sz.nelem, A.status + sg.model)) return;
         const Band b = A.bands[sg.table + lo];
         const int64_t np = i - b.first;
         double phi = b.phi1 + (b.phi2 - b.phi1) * ((double)np + 0.5) / (double)b.nphi;
@@ -723,6 +737,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
             int mid = (lo + hi + 1) >> 1;
             if (A.rings[sg.table + mid].first <= i) lo = mid; else hi = mid - 1;
         }
+        if (!LCB_IN_BOUNDS(sg.table + lo < A.sz.nrings && sg.first + i < A.sz.nelem, A.status + sg.model)) return;
         const Ring g = A.rings[sg.table + lo];
         double th = kTwoPi * (double)(i - g.first) / (double)g.ntheta;
         double st, ct;
@@ -783,6 +798,7 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
         else { dx = 0.0; dy = 0.0; dz = 1.0; flux = (float)(bright * M.cfrac_spot * M.area_spot); }
     }
     const int64_t e = sg.first + i;
+    if (!LCB_IN_BOUNDS(e < A.sz.nelem, A.status + sg.model)) return;
     A.el_rec[e] = make_float4((float)dx, (float)dy, (float)dz, flux);
     A.el_pos[e] = make_float4((float)px, (float)py, (float)pz, 0.f);
     A.el_p64[e] = make_double4(px, py, pz, (double)area);
@@ -803,7 +819,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs
     EclCount cnt;
     cnt.cap = A.fblink_cap;
     bool capped = false;
-    if (i < sg.count) {
+    if (i < sg.count && LCB_IN_BOUNDS(sg.first + i < A.sz.nelem, A.status + sg.model)) {
         const ModelDev& M = A.models[sg.model];
         const int by = blk.by;
         const int64_t e = sg.first + i;
@@ -830,7 +846,7 @@ __device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double d
     for (int i = lo; i < hi; ++i) {
         if (((i - lo) & 7) == 0 && *(volatile int*)first < lo) return;
         earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
-        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget > 0);
+        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget);
         if (capped) return;
         if (hit) {
             atomicMin(first, i);
@@ -862,7 +878,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(Ele
     EclCount cnt;
     cnt.cap = A.fblink_cap;
     bool capped = false;
-    if (i < sg.count) {
+    if (i < sg.count && LCB_IN_BOUNDS(sg.first + i < A.sz.nelem, A.status + sg.model)) {
         const ModelDev& M = A.models[sg.model];
         const double4 p = A.el_p64[sg.first + i];
         scan_chunk(blk.by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, chunk, A.roche_split,
@@ -890,7 +906,8 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(El
     bool capped = false, found = false;
     double a = 0.0, b = 0.0;
     int64_t e = 0;
-    if (i < sg.count) {
+    const bool valid = i < sg.count && LCB_IN_BOUNDS(sg.first + i < A.sz.nelem, A.status + sg.model);
+    if (valid) {
         const ModelDev& M = A.models[sg.model];
         const RocheEcl& R = blk.by == 1 ? M.ecl1 : M.ecl2;
         e = sg.first + i;
@@ -904,7 +921,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(El
     const double egress = __shfl_xor_sync(0xffffffffu, b, 1);
     const bool found_eg = __shfl_xor_sync(0xffffffffu, (int)found, 1) != 0;
     const bool capped_eg = __shfl_xor_sync(0xffffffffu, (int)capped, 1) != 0;
-    if (i < sg.count && part == 0) {
+    if (valid && part == 0) {
         if (found && found_eg) A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, blk.by)] =
             make_double2(a, egress < a ? egress + 1.0 : egress);
         if (capped || capped_eg) atomicOr(A.status + sg.model, kStatusIterCap);
@@ -921,7 +938,7 @@ __global__ void __launch_bounds__(kElemThreads) k_aux(ElemArgs A) {
     const SegDesc sg = A.segs[blk.seg];
     const ModelDev& M = A.models[sg.model];
     const int64_t i = blk.offset + threadIdx.x;
-    const bool valid = i < sg.count;
+    const bool valid = i < sg.count && LCB_IN_BOUNDS(sg.first + i < A.sz.nelem, A.status + sg.model);
     const int star = sg.kind == SEG_STAR1 ? 1 : 2;
     double px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 0, area = 0, grav = 0, flux = 0;
     double2 ecl[kMaxEcl];
@@ -1481,6 +1498,12 @@ __global__ void __launch_bounds__(kFluxThreads, 5) k_flux(FluxArgs A) {
         __syncthreads();
         if (u >= A.nunits) break;
         const FluxUnit U = A.units[u];
+        if (!LCB_IN_BOUNDS(U.e0 + U.ne <= A.sz.nelem &&
+                               A.models[U.model].sub_begin + U.t0 + U.nt <= A.sz.nsub &&
+                               A.models[U.model].pbase + (int64_t)(U.slot + 1) * A.models[U.model].nsub <=
+                                   A.sz.npartial,
+                           A.status + U.model))
+            continue;  // the unit is skipped by the whole block
         switch (U.kind) {
             case UK_STAR_POLY1: flux_unit<UK_STAR_POLY1>(A, U, S, parity); break;
             case UK_STAR_POLY2: flux_unit<UK_STAR_POLY2>(A, U, S, parity); break;
@@ -1684,7 +1707,10 @@ __global__ void __launch_bounds__(kEpiThreads) k_epilogue(EpiArgs A) {
     __shared__ double red[kEpiThreads / 32];
     __shared__ Gint G;
     __shared__ double s_wd;
-    if (M.status < 0 || A.status[m] != 0) {
+    const bool in_range = LCB_IN_BOUNDS(M.pbase + (int64_t)M.nslots * M.nsub <= A.sz.npartial &&
+                                            M.datum_begin + M.ndatum <= A.sz.ndatum && M.sub_begin + M.nsub <= A.sz.nsub,
+                                        A.bad + m);
+    if (M.status < 0 || A.status[m] != 0 || !in_range) {
         if (threadIdx.x == 0) {
             for (int k = 0; k < 12; ++k) res[k] = NAN;
         }

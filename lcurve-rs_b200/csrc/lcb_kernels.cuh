@@ -8,6 +8,11 @@
 
 namespace lcb {
 
+// Sizes of the batch's arrays, for the index checks of the LCURVE_DEBUG_BOUNDS build.
+struct Sizes {
+    int64_t nelem, nsub, npartial, ndatum, nbands, nrings;
+};
+
 struct ElemArgs {
     const ModelDev* models;
     const SegDesc* segs;
@@ -28,6 +33,7 @@ struct ElemArgs {
     int roche_split;     // threads per Roche-eclipsed element in the phase scan (1: one kernel)
     int* firsthit;       // split scan: first hit per Roche thread (nrblocks x kRocheBlock), starts at 0x7f7f7f7f
     int fblink_cap;      // potential evaluations allowed in one line-of-sight search (kFblinkEvalCap)
+    Sizes sz;
 };
 
 struct PhaseArgs {
@@ -56,6 +62,7 @@ struct FluxArgs {
     const int8_t* sp_type;
     double* partial;
     int* status;         // per model
+    Sizes sz;
 };
 
 struct EpiArgs {
@@ -74,6 +81,8 @@ struct EpiArgs {
     double* fcomp;       // iscale: 5 component fluxes per datum
     double* svda;        // iscale: 5 per datum, the weighted design matrix of the scale fit
     int64_t nmodels;
+    Sizes sz;
+    int* bad;            // LCURVE_DEBUG_BOUNDS: per-model status words the epilogue may set
 };
 
 size_t flux_smem_bytes();
