@@ -140,10 +140,14 @@ struct EclCount {
 
 // dbrent with stop-fast (crates/subs/src/numerical/dbrent.rs:20-165).
 // Returns 1 = bracketed minimum below fref, 0 = not below.
+// `local` counts the search's evaluations so far; past cnt.cap the search stops
+// and sets `capped` (the model then fails).
 __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double bx, double cx, double acc,
-                             double fref, EclCount& cnt) {
+                             double fref, EclCount& cnt, int& local, bool& capped) {
     double a = fmin(ax, cx), b = fmax(ax, cx);
     double x = bx, w = bx, v = bx;
+    if (local + 2 > cnt.cap) { capped = true; return false; }
+    local += 2;
     double fx = los_pot(s, L, x), fw = fx, fv = fx;
     ++cnt.pot;
     if (fx < fref) return true;
@@ -181,6 +185,8 @@ __device__ bool dbrent_below(const RocheEcl& s, const Los& L, double ax, double 
             d = 0.5 * e;
         }
         double u, fu;
+        if (local + 2 > cnt.cap) { capped = true; return false; }
+        local += 2;
         if (fabs(d) >= tol1) {
             u = x + d;
             fu = los_pot(s, L, u);
@@ -331,7 +337,7 @@ __device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L,
         }
     }
     cnt.pot += local;
-    if (br) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, cnt);
+    if (br) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, cnt, local, capped);
     return false;
 }
 
