@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <deque>
@@ -748,7 +750,78 @@ int64_t host_numface(int nlat) {
     return star_bands(m, true, nlat, false, 0, 0, 0, 0, b);
 }
 
+// A process-wide pool of host threads for the planner: a parallel loop
+// publishes its index range as a job, the calling thread works on it too, and
+// idle workers take indices from any open job, so small batches (an MCMC step
+// plans a few models) pay no thread start-up per call.  Several contexts may
+// plan at once: jobs are independent.
+class HostPool {
+    struct Job {
+        const std::function<void(int64_t)>* f = nullptr;
+        int64_t n = 0;
+        std::atomic<int64_t> next{0}, done{0};
+        int helpers = 0, users = 0;  // workers allowed / working on it (under the pool mutex)
+    };
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::vector<Job*> open_;
+
+    Job* pick() {
+        for (Job* j : open_)
+            if (j->users < j->helpers && j->next.load() < j->n) { ++j->users; return j; }
+        return nullptr;
+    }
+    void work(Job* j) {
+        for (int64_t i; (i = j->next.fetch_add(1)) < j->n;) {
+            (*j->f)(i);
+            if (j->done.fetch_add(1) + 1 == j->n) {
+                std::lock_guard<std::mutex> g(mu_);
+                cv_.notify_all();
+            }
+        }
+    }
+
+public:
+    const int size;
+    explicit HostPool(int workers) : size(workers) {
+        for (int t = 0; t < workers; ++t)
+            std::thread([this] {
+                for (;;) {
+                    Job* j = nullptr;
+                    {
+                        std::unique_lock<std::mutex> lk(mu_);
+                        cv_.wait(lk, [&] { return (j = pick()) != nullptr; });
+                    }
+                    work(j);
+                    std::lock_guard<std::mutex> g(mu_);
+                    if (--j->users == 0) cv_.notify_all();
+                }
+            }).detach();  // process-lifetime workers
+    }
+    static HostPool& get() {
+        static HostPool* p = new HostPool((int)std::max(1u, std::thread::hardware_concurrency()) - 1);
+        return *p;
+    }
+    void run(int64_t n, int helpers, const std::function<void(int64_t)>& f) {
+        Job j;
+        j.f = &f;
+        j.n = n;
+        j.helpers = helpers;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            open_.push_back(&j);
+        }
+        cv_.notify_all();
+        work(&j);
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return j.done.load() == n; });
+        open_.erase(std::find(open_.begin(), open_.end(), &j));
+        cv_.wait(lk, [&] { return j.users == 0; });
+    }
+};
+
 // Runs f(0..n) on the host's cores (items of `grain` or more per thread).
+// f must not throw.
 template <class F>
 void parallel_for(int64_t n, int64_t grain, F&& f) {
     const int64_t nthreads =
@@ -757,13 +830,8 @@ void parallel_for(int64_t n, int64_t grain, F&& f) {
         for (int64_t i = 0; i < n; ++i) f(i);
         return;
     }
-    std::atomic<int64_t> next{0};
-    std::vector<std::thread> pool;
-    for (int64_t t = 0; t < nthreads; ++t)
-        pool.emplace_back([&] {
-            for (int64_t i; (i = next.fetch_add(1)) < n;) f(i);
-        });
-    for (auto& t : pool) t.join();
+    const std::function<void(int64_t)> fn = [&](int64_t i) { f(i); };
+    HostPool::get().run(n, (int)nthreads - 1, fn);
 }
 
 void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, const int64_t* start,
@@ -807,8 +875,8 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             }
         });
     }
-    // models are independent: prepare them on the host's cores (8 or more per thread)
-    parallel_for(n, 8, prep);
+    // models are independent: prepare them on the host's cores (~40 us each)
+    parallel_for(n, 1, prep);
     // sub-phases and data: per-model sums, prefix offsets, then the per-datum
     // arrays of each model filled in parallel
     std::vector<int64_t> dbeg(n + 1, 0), sbeg(n + 1, 0);

@@ -60,13 +60,15 @@ def test_search_cap_fails_the_roche_models_and_the_default_recovers(lcb):
         assert np.array_equal(sphere.light_curve(times=t, expose=0.001, ndiv=1).flux, base)
         B.run(scale=False)  # the resident batch's graph is captured again with the lowered cap
         bchi, _, _ = B.results()
-        assert np.isnan(bchi[0]) and bchi[1] == ok_chi[1]
+        assert np.isnan(bchi[0]) and bchi[1] == pytest.approx(ok_chi[1], rel=1e-12)
     finally:
         lcb._capi.check(L.lcb_ctx_set_search_cap(ctx, 0))
-    assert np.array_equal(roche.light_curve(times=t, expose=0.001, ndiv=1).flux, good)
+    # restored: the results before (the per-model sums behind the ginterp scale factors are
+    # FP64 atomics, so the last bits may differ from run to run)
+    assert np.allclose(roche.light_curve(times=t, expose=0.001, ndiv=1).flux, good, rtol=1e-12, atol=0)
     B.run(scale=False)
     bchi, _, _ = B.results()
-    assert np.array_equal(bchi, ok_chi)
+    assert np.allclose(bchi, ok_chi, rtol=1e-12, atol=0)
     g = np.loadtxt(GOLDEN / "test_lc.dat")
     r = lcb.Model(GOLDEN / "test_model.dat").light_curve(time1=-0.2, time2=1.2, ntime=500, expose=0.001, ndiv=1)
     assert np.max(np.abs(r.flux - g[:, 2]) / np.abs(g[:, 2])) < 1e-5
