@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--mcmc-burn", type=int, default=500)
     p.add_argument("--mcmc-substeps", type=int, default=2)
     p.add_argument("--mcmc-bandwidth", type=float, default=0.6, help="KDE bandwidth in units of Scott's factor")
+    p.add_argument("--mcmc-refine", type=int, default=262144,
+                   help="curves for sharpening the surrogate near the burned-in ensemble (0: none)")
     p.add_argument("--autotune", action="store_true",
                    help="tune the resident batch's launch shapes (lcurve-rs_b200/autotune.py) before timing")
     p.add_argument("--train-profile", type=int, default=0, metavar="K",
@@ -370,6 +372,7 @@ def run_mcmc(args, lcb):
     gen_s = time.perf_counter() - t0
     sur = S.Surrogate()
     losses = sur.fit(theta[:n], curves[:n], epochs=args.mcmc_epochs)
+    train_global_s = sur.train_seconds
     ok = np.isfinite(curves[n:]).all(axis=1)
     rel = S.scaled_rel_error(sur.predict(theta[n:][ok]), curves[n:][ok])
 
@@ -380,6 +383,12 @@ def run_mcmc(args, lcb):
     p0 = M.initial_walkers(256, S.TRUTH, seed=3)
     burn = M.run_delayed(eng, sur, p0, args.mcmc_burn, seed=4, substeps=32)
     start = burn.chain[-1]
+    sample = start[:128]
+    dchi_global = eng.chisq(sample) - sur.chisq(sample)
+    refine_s = 0.0
+    if args.mcmc_refine:  # more training where the sampler sits; the samplers stay exact
+        refine_s = S.refine_near(sur, setup, start, theta[:n], curves[:n], n=args.mcmc_refine, widen=2.5,
+                                 epochs=100, lr=1e-3)
     bw, k = args.mcmc_bandwidth, args.mcmc_substeps
     runs = {
         "plain_stretch": M.run_plain(eng, start, args.mcmc_steps, seed=5),
@@ -391,9 +400,8 @@ def run_mcmc(args, lcb):
     post = {name: M.posterior_summary(r, burn=0.0) for name, r in runs.items()}
     ref = post["plain_stretch"]
     shift = {name: max(abs(p[q][0] - ref[q][0]) / ref[q][1] for q in ref) for name, p in post.items()}
-    sample = start[:128]
     dchi = eng.chisq(sample) - sur.chisq(sample)
-    overhead = gen_s + sur.train_seconds
+    overhead = gen_s + train_global_s + refine_s  # curves, training and refinement
     return {
         "ess_per_s": rate,
         "speedup_vs_plain_stretch": rate["da_kde"] / rate["plain_stretch"],
@@ -402,7 +410,7 @@ def run_mcmc(args, lcb):
         "ess": {name: e[0] for name, e in ess.items()},
         "tau": {name: e[1].tolist() for name, e in ess.items()},
         "seconds": {**{name: r.seconds for name, r in runs.items()}, "curve_generation": gen_s,
-                    "training": sur.train_seconds, "burn_in": burn.seconds},
+                    "training": train_global_s, "refine": refine_s, "burn_in": burn.seconds},
         "engine_evals": {name: r.engine_evals for name, r in runs.items()},
         "acceptance": {name: r.acceptance for name, r in runs.items()},
         "posterior": post, "max_mean_shift_vs_plain_stretch_in_sigma": shift,
@@ -410,7 +418,12 @@ def run_mcmc(args, lcb):
                       "train_curves": n, "epochs": args.mcmc_epochs, "final_loss": losses[-1],
                       "holdout_scaled_rel_err": {"median": float(np.median(rel)),
                                                  "p99": float(np.quantile(rel, 0.99)), "max": float(rel.max())},
-                      "posterior_chisq_minus_engine": {"mean": float(-dchi.mean()), "std": float(dchi.std())}},
+                      "posterior_chisq_minus_engine": {"mean": float(-dchi.mean()), "std": float(dchi.std())},
+                      "posterior_chisq_minus_engine_before_refine": {"mean": float(-dchi_global.mean()),
+                                                                     "std": float(dchi_global.std())},
+                      "refine": {"curves": args.mcmc_refine, "seconds": refine_s,
+                                 "how": "Gaussian of the burned-in ensemble, covariance x 2.5^2, 100 epochs mixed "
+                                        "with as many global rows (surrogate.refine_near)"}},
         "config": {"walkers": 256, "steps": args.mcmc_steps, "burn_in_steps": args.mcmc_burn,
                    "da_substeps": k, "kde_bandwidth_x_scott": bw, "phases": setup.n_phase, "stretch_a": 2.0,
                    "likelihood": "-chisq/2, chisq_batch scale=True, uniform prior box of the 1024-model batch",

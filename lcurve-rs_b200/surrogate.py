@@ -164,7 +164,10 @@ class Surrogate:
     """The MLP, its input/output normalisation, training and inference."""
 
     def __init__(self, n_phase: int = 256, width: int = 512, n_hidden: int = 4, max_batch: int = 8192, seed: int = 0,
-                 device: int = 0):
+                 device: int = 0, box: tuple | None = None):
+        """box = (lo, hi): the parameter box the inputs are scaled to [-1, 1]
+        over (default the prior box); a local surrogate uses a small one.
+        Proposals outside the prior box are rejected either way."""
         torch = _torch()
         self.L = _capi.load()
         self.n_phase, self.width, self.n_hidden = n_phase, width, n_hidden
@@ -182,12 +185,15 @@ class Surrogate:
         # the same input map for the device sub-chain: fadd + fmul * (x or 1/x)
         d = len(PARAMS)
         recip = [0, 0, 0, 1, 1]
-        span = FEAT_HI - FEAT_LO
+        self.box = (np.array(PRIOR_LO), np.array(PRIOR_HI)) if box is None else (np.array(box[0]), np.array(box[1]))
+        f = features(np.vstack(self.box))
+        flo, fhi = f.min(axis=0), f.max(axis=0)
+        span = fhi - flo
         self._c_lo = (C.c_double * d)(*PRIOR_LO)
         self._c_hi = (C.c_double * d)(*PRIOR_HI)
         self._c_recip = (C.c_int * d)(*recip)
         self._c_fmul = (C.c_float * d)(*[2.0 / span[k] * (HC_OVER_LK if recip[k] else 1.0) for k in range(d)])
-        self._c_fadd = (C.c_float * d)(*[-2.0 * FEAT_LO[k] / span[k] - 1.0 for k in range(d)])
+        self._c_fadd = (C.c_float * d)(*[-2.0 * flo[k] / span[k] - 1.0 for k in range(d)])
         self._recip = np.array(recip, dtype=bool)
         self._fmul64 = np.array(self._c_fmul, dtype=np.float32).astype(np.float64)
         self._fadd64 = np.array(self._c_fadd, dtype=np.float32).astype(np.float64)
@@ -298,14 +304,15 @@ class Surrogate:
                                                  C.byref(steps)))
         np.savez(path, state=state, steps=steps.value, mean=self.mean.cpu().numpy(), sd=self.sd.cpu().numpy(),
                  shape=np.array([self.n_phase, self.width, self.n_hidden, self.max_batch]),
-                 train_seconds=self.train_seconds)
+                 train_seconds=self.train_seconds, box=np.vstack(self.box))
 
     @classmethod
     def load(cls, path, device: int = 0) -> "Surrogate":
         torch = _torch()
         with np.load(path) as z:
             n_phase, width, n_hidden, max_batch = (int(v) for v in z["shape"])
-            sur = cls(n_phase=n_phase, width=width, n_hidden=n_hidden, max_batch=max_batch, device=device)
+            sur = cls(n_phase=n_phase, width=width, n_hidden=n_hidden, max_batch=max_batch, device=device,
+                      box=tuple(z["box"]) if "box" in z.files else None)
             state = np.ascontiguousarray(z["state"], dtype=np.float32)
             _capi.check_mlp(sur.L.lcb_mlp_set_state(sur._h, C.c_void_p(state.ctypes.data), state.size,
                                                     int(z["steps"])))
@@ -447,3 +454,27 @@ def refine_near(sur: Surrogate, setup: CurveSetup, ensemble: np.ndarray, theta_g
     flux = np.concatenate([curves, flux_global[pick]])
     sur.fit(theta, flux, epochs=epochs, lr=lr, lr_min=lr * 0.01, log=log, renormalize=False)
     return time.perf_counter() - t0
+
+
+def local_surrogate(setup: CurveSetup, ensemble: np.ndarray, n: int = 262144, widen: float = 4.0,
+                    epochs: int = 200, seed: int = 11, data=None, log=None) -> tuple["Surrogate", float]:
+    """A second network for where a sampler's ensemble sits: trained from
+    scratch on n engine curves drawn from a Gaussian with the ensemble's mean
+    and covariance widened by `widen` (inside the prior box), its inputs
+    scaled over that region (the ensemble's range widened likewise), so the
+    same network resolves the curve's small variations there.  The sampler
+    that uses it stays exact (delayed acceptance), and it still rejects
+    proposals outside the prior box.  Returns (surrogate, seconds)."""
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    mu = ensemble.mean(axis=0)
+    cov = np.cov(ensemble, rowvar=False) * widen ** 2 + np.diag(1e-12 * (PRIOR_HI - PRIOR_LO) ** 2)
+    theta = rng.multivariate_normal(mu, cov, size=2 * n)
+    theta = theta[np.all((theta >= PRIOR_LO) & (theta <= PRIOR_HI), axis=1)][:n]
+    lo, hi = theta.min(axis=0), theta.max(axis=0)
+    curves = generate_curves(setup, theta)
+    sur = Surrogate(box=(lo, hi))
+    sur.fit(theta, curves, epochs=epochs, log=log)
+    if data is not None:
+        sur.bind_data(data)
+    return sur, time.perf_counter() - t0
