@@ -557,17 +557,21 @@ struct StretchArgs {
                            // parameter, so one captured graph serves every half-step
 };
 
-// log of the Gaussian KDE of the complementary walkers at v (up to a constant):
-// log sum_j exp(-(v - c_j)^T prec (v - c_j) / 2), accumulated with a running maximum.
-__device__ double kde_logq(const StretchArgs& A, const double* v) {
+// log of the Gaussian KDE of the complementary walkers at v (up to a constant),
+// log sum_j exp(-(v - c_j)^T prec (v - c_j) / 2), computed by one warp: each lane
+// takes every 32nd component, then a log-sum-exp across the warp.  Every lane
+// returns the value.
+__device__ double kde_logq_warp(const StretchArgs& A, const double* v) {
+    const int lane = threadIdx.x & 31;
+    const double* prec = A.kde + kMaxDim * kMaxDim;
     double mx = -INFINITY, acc = 0.0;
-    for (int j = 0; j < A.m; ++j) {
+    for (int j = lane; j < A.m; j += 32) {
         double dv[kMaxDim];
         for (int k = 0; k < A.d; ++k) dv[k] = v[k] - A.comp[(size_t)j * A.d + k];
         double qf = 0.0;
         for (int k = 0; k < A.d; ++k) {
             double t = 0.0;
-            for (int l = 0; l < A.d; ++l) t += A.kde[kMaxDim * kMaxDim + k * kMaxDim + l] * dv[l];
+            for (int l = 0; l < A.d; ++l) t += prec[k * kMaxDim + l] * dv[l];
             qf += dv[k] * t;
         }
         const double e = -0.5 * qf;
@@ -578,45 +582,61 @@ __device__ double kde_logq(const StretchArgs& A, const double* v) {
             acc += exp(e - mx);
         }
     }
-    return mx + log(acc);
+    double wmx = mx;
+    for (int o = 16; o > 0; o >>= 1) wmx = fmax(wmx, __shfl_xor_sync(0xffffffffu, wmx, o));
+    double part = mx == -INFINITY ? 0.0 : acc * exp(mx - wmx);
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    return wmx + log(part);
 }
 
+constexpr int kWalkersPerBlock = 4;  // one warp per walker in the KDE kernels
+
 __global__ void k_kde_logq(StretchArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n || A.move != MOVE_KDE) return;
+    const int i = blockIdx.x * kWalkersPerBlock + (threadIdx.x >> 5);
+    if (i >= A.n || A.move != MOVE_KDE) return;  // uniform per warp
     double v[kMaxDim];
     for (int k = 0; k < A.d; ++k) v[k] = A.y[(size_t)i * A.d + k];
-    A.lq[i] = kde_logq(A, v);
+    const double lq = kde_logq_warp(A, v);
+    if ((threadIdx.x & 31) == 0) A.lq[i] = lq;
+}
+
+// KDE move (emcee's KDEMove): an independence proposal from the Gaussian KDE
+// of the complementary walkers, y' = c_j + chol eps, for walker i (one warp);
+// writes y', its network inputs and the log density ratio log q(y) - log q(y'),
+// or -inf outside the prior box.
+__global__ void k_kde_propose(StretchArgs A, int step) {
+    const int i = blockIdx.x * kWalkersPerBlock + (threadIdx.x >> 5);
+    if (i >= A.n) return;  // uniform per warp
+    const bool lead = (threadIdx.x & 31) == 0;
+    const double* r = A.rnd + ((size_t)step * A.n + i) * A.rstride;
+    const int j = min((int)(r[0] * A.m), A.m - 1);
+    double v[kMaxDim];
+    bool inside = true;
+    for (int k = 0; k < A.d; ++k) {
+        double t = 0.0;
+        for (int l = 0; l <= k; ++l) t += A.kde[k * kMaxDim + l] * r[3 + l];
+        v[k] = A.comp[(size_t)j * A.d + k] + t;
+        inside = inside && v[k] >= A.lo[k] && v[k] <= A.hi[k];
+        if (lead) {
+            A.yp[(size_t)i * A.d + k] = v[k];
+            const double f = A.frecip[k] ? 1.0 / v[k] : v[k];
+            A.xin[(size_t)i * A.n_in + k] = (float)__dadd_rn((double)A.fadd[k], __dmul_rn((double)A.fmul[k], f));
+        }
+    }
+    const double lqp = kde_logq_warp(A, v);
+    if (lead) {
+        A.lqp[i] = lqp;
+        A.lz[i] = inside ? A.lq[i] - lqp : -INFINITY;
+    }
 }
 
 // Goodman & Weare stretch proposal y' = c + z (y - c), z ~ g(z) on [1/a, a];
-// the network input of y' is fadd + fmul * (y' or 1/y') per dimension.
-//
-// KDE move (emcee's KDEMove): an independence proposal from the Gaussian KDE of
-// the complementary walkers, y' = c_j + chol eps, with log density ratio
-// log q(y) - log q(y').
+// the network input of y' is fadd + fmul * (y' or 1/y') per dimension.  (The
+// KDE move, emcee's KDEMove, is k_kde_propose above.)
 __global__ void k_stretch_propose(StretchArgs A, int step) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     const double* r = A.rnd + ((size_t)step * A.n + i) * A.rstride;
-    if (A.move == MOVE_KDE) {
-        const int j = min((int)(r[0] * A.m), A.m - 1);
-        double v[kMaxDim];
-        bool inside = true;
-        for (int k = 0; k < A.d; ++k) {
-            double t = 0.0;
-            for (int l = 0; l <= k; ++l) t += A.kde[k * kMaxDim + l] * r[3 + l];
-            v[k] = A.comp[(size_t)j * A.d + k] + t;
-            A.yp[(size_t)i * A.d + k] = v[k];
-            inside = inside && v[k] >= A.lo[k] && v[k] <= A.hi[k];
-            const double f = A.frecip[k] ? 1.0 / v[k] : v[k];
-            A.xin[(size_t)i * A.n_in + k] = (float)__dadd_rn((double)A.fadd[k], __dmul_rn((double)A.fmul[k], f));
-        }
-        const double lqp = kde_logq(A, v);
-        A.lqp[i] = lqp;
-        A.lz[i] = inside ? A.lq[i] - lqp : -INFINITY;
-        return;
-    }
     // explicitly rounded operations (no contraction), so the moves are the
     // ones a host implementation of the same formulas makes
     double z = __dadd_rn(__dmul_rn(A.a - 1.0, r[0]), 1.0);
@@ -1288,12 +1308,14 @@ int lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y_
         }
         auto enqueue = [&] {
             const unsigned g = (unsigned)((n + 127) / 128);
+            const unsigned gw = (unsigned)((n + kWalkersPerBlock - 1) / kWalkersPerBlock);  // a warp per walker
             if (move == MOVE_KDE) {
-                k_kde_logq<<<g, 128, 0, st>>>(A);
+                k_kde_logq<<<gw, 32 * kWalkersPerBlock, 0, st>>>(A);
                 CK(cudaGetLastError());
             }
             for (int k = 0; k < steps; ++k) {
-                k_stretch_propose<<<g, 128, 0, st>>>(A, k);
+                if (move == MOVE_KDE) k_kde_propose<<<gw, 32 * kWalkersPerBlock, 0, st>>>(A, k);
+                else k_stretch_propose<<<g, 128, 0, st>>>(A, k);
                 CK(cudaGetLastError());
                 net->forward(net->sub_x.p, n, nullptr);
                 k_logflux_chisq<<<(unsigned)n, 128, 0, st>>>((int)n, net->n_out, net->pred.p, mean_dev, sd_dev,
