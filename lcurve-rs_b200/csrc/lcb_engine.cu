@@ -74,11 +74,11 @@ struct DevBuf {
 // All device storage of one planned batch.
 struct DeviceSet {
     DevBuf models, segs, bands, rings, eblocks, rblocks, ablocks, units, dmodel, dsub0, dsrc, data;
-    DevBuf rec, pos, p64, d64, ecl, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter,
+    DevBuf rec, pos, p64, d64, ecl, egrp, aux, status, spe, spphi, sptype, spw, slfac, partial, calc, results, counter,
         datum, ecount, fcomp, svda, firsthit;
     void release() {
         for (DevBuf* b : {&models, &segs, &bands, &rings, &eblocks, &rblocks, &ablocks, &units, &dmodel, &dsub0, &dsrc,
-                          &data, &rec, &pos, &p64, &d64, &ecl, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac,
+                          &data, &rec, &pos, &p64, &d64, &ecl, &egrp, &aux, &status, &spe, &spphi, &sptype, &spw, &slfac,
                           &partial, &calc, &results, &counter, &datum, &ecount, &fcomp, &svda, &firsthit})
             b->release();
     }
@@ -132,6 +132,9 @@ struct lcb_batch {
 namespace {
 
 // Upload of the plan's tables (and the data) into a device set.
+// Words of the per-group eclipse slot masks (one per kEclGroup elements).
+size_t ecl_groups(const lcb::Plan& P) { return (size_t)((P.nelem + lcb::kEclGroup - 1) / lcb::kEclGroup); }
+
 void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* data, int64_t ndata_src,
                  bool upload_data) {
     cudaStream_t s = C->stream;
@@ -170,6 +173,7 @@ void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* 
     D.p64.ensure(P.nelem * sizeof(double4));
     D.d64.ensure(P.nelem * sizeof(double4));
     D.ecl.ensure(P.nelem * lcb::kMaxEcl * sizeof(double2));
+    D.egrp.ensure(ecl_groups(P) * sizeof(unsigned));
     D.aux.ensure(nm * lcb::kNumAux * sizeof(double));
     D.status.ensure(nm * sizeof(int));
     D.spe.ensure(P.nsub * sizeof(float4));
@@ -216,10 +220,11 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     lcb::ElemArgs ea{D.models.as<lcb::ModelDev>(), D.segs.as<lcb::SegDesc>(), D.eblocks.as<lcb::ElemBlock>(),
                      D.rblocks.as<lcb::ElemBlock>(), D.ablocks.as<lcb::ElemBlock>(), D.bands.as<lcb::Band>(),
                      D.rings.as<lcb::Ring>(), D.rec.as<float4>(), D.pos.as<float4>(), D.p64.as<double4>(),
-                     D.d64.as<double4>(), D.ecl.as<double2>(), D.aux.as<double>(), D.status.as<int>(),
-                     nblk, nrblk, (int64_t)P.ablocks.size(),
+                     D.d64.as<double4>(), D.ecl.as<double2>(), D.egrp.as<unsigned>(), D.aux.as<double>(),
+                     D.status.as<int>(), nblk, nrblk, (int64_t)P.ablocks.size(),
                      D.ecount.as<unsigned long long>(), P.roche_split, D.firsthit.as<int>(), C->fblink_cap, sz};
     if (elem) {
+        CUDA_TRY(cudaMemsetAsync(D.egrp.p, 0, ecl_groups(P) * sizeof(unsigned), s));
         if (P.roche_split > 1 && nrblk > 0)
             CUDA_TRY(cudaMemsetAsync(D.firsthit.p, 0x7f, nrblk * lcb::kRocheBlock * sizeof(int), s));
         CUDA_TRY(lcb::launch_elements(ea, s));
@@ -232,7 +237,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
     if (timed) CUDA_TRY(cudaEventRecord(C->ev[4], s));
     lcb::FluxArgs fa{D.models.as<lcb::ModelDev>(), D.units.as<lcb::FluxUnit>(), (int64_t)P.units.size(),
                      D.counter.as<int>(), D.rec.as<float4>(), D.pos.as<float4>(), D.ecl.as<double2>(),
-                     D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
+                     D.egrp.as<unsigned>(), D.spe.as<float4>(), D.spphi.as<double>(), D.sptype.as<int8_t>(), D.partial.as<double>(),
                      D.status.as<int>(), sz};
     const int bps_max = lcb::flux_blocks_per_sm();
     const int bps = P.flux_blocks_per_sm > 0 ? std::min(P.flux_blocks_per_sm, bps_max) : bps_max;
@@ -543,8 +548,9 @@ int lcb_model_grid(lcb_ctx* C, const lcb_model* model, int which, int64_t* n, do
                             cudaMemcpyDeviceToHost));
         CUDA_TRY(cudaMemcpy(rec.data(), C->scratch.rec.as<float4>() + g->first, g->count * sizeof(float4),
                             cudaMemcpyDeviceToHost));
-        CUDA_TRY(cudaMemcpy(e.data(), C->scratch.ecl.as<double2>() + g->first * lcb::kMaxEcl,
-                            e.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < lcb::kMaxEcl; ++k)  // slot-major on the device
+            CUDA_TRY(cudaMemcpy(e.data() + k * g->count, C->scratch.ecl.as<double2>() + k * P.nelem + g->first,
+                                g->count * sizeof(double2), cudaMemcpyDeviceToHost));
         for (int64_t i = 0; i < g->count; ++i) {
             posn[3 * i] = p64[i].x; posn[3 * i + 1] = p64[i].y; posn[3 * i + 2] = p64[i].z;
             if (dirn) { dirn[3 * i] = d64[i].x; dirn[3 * i + 1] = d64[i].y; dirn[3 * i + 2] = d64[i].z; }
@@ -553,20 +559,17 @@ int lcb_model_grid(lcb_ctx* C, const lcb_model* model, int which, int64_t* n, do
             if (flux) flux[i] = rec[i].w;
             if (ecl)
                 for (int k = 0; k < lcb::kMaxEcl; ++k) {
-                    ecl[8 * i + 2 * k] = e[i * lcb::kMaxEcl + k].x;
-                    ecl[8 * i + 2 * k + 1] = e[i * lcb::kMaxEcl + k].y;
+                    ecl[8 * i + 2 * k] = e[k * g->count + i].x;
+                    ecl[8 * i + 2 * k + 1] = e[k * g->count + i].y;
                 }
         }
     });
 }
 
 // Element records of one model exchanged across devices (a model split into element slabs):
-// five device arrays in the engine's own layout and order.
-struct ElemViews {
-    void* rec; void* pos; void* p64; void* d64; void* ecl;
-};
-static const size_t kElemBytes[5] = {sizeof(float4), sizeof(float4), sizeof(double4), sizeof(double4),
-                                     lcb::kMaxEcl * sizeof(double2)};
+// five device arrays in the engine's own element order; the eclipse slots element-major
+// (kMaxEcl pairs per element), converted from and to the engine's slot-major array.
+static const size_t kElemBytes[4] = {sizeof(float4), sizeof(float4), sizeof(double4), sizeof(double4)};
 
 int lcb_model_elements(lcb_ctx* C, const lcb_model* model, int64_t first, int64_t count, void* rec_dev,
                        void* pos_dev, void* p64_dev, void* d64_dev, void* ecl_dev, int64_t* total) {
@@ -605,11 +608,12 @@ int lcb_model_elements(lcb_ctx* C, const lcb_model* model, int64_t first, int64_
             CUDA_TRY(cudaMemcpyAsync(D.rblocks.p, rb.data(), rb.size() * sizeof(lcb::ElemBlock),
                                      cudaMemcpyHostToDevice, C->stream));
         enqueue_run(C, D, P, 0, 0, false, kStageElements, (int64_t)eb.size(), (int64_t)rb.size());
-        void* dst[5] = {rec_dev, pos_dev, p64_dev, d64_dev, ecl_dev};
-        const void* src[5] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p, D.ecl.p};
-        for (int k = 0; k < 5; ++k)
+        void* dst[4] = {rec_dev, pos_dev, p64_dev, d64_dev};
+        const void* src[4] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p};
+        for (int k = 0; k < 4; ++k)
             CUDA_TRY(cudaMemcpyAsync(dst[k], (const char*)src[k] + first * kElemBytes[k], count * kElemBytes[k],
                                      cudaMemcpyDeviceToDevice, C->stream));
+        CUDA_TRY(lcb::launch_ecl_export(D.ecl.as<double2>(), P.nelem, first, count, (double2*)ecl_dev, C->stream));
         int status = 0;
         CUDA_TRY(cudaMemcpyAsync(&status, D.status.p, sizeof(int), cudaMemcpyDeviceToHost, C->stream));
         CUDA_TRY(cudaStreamSynchronize(C->stream));
@@ -633,11 +637,14 @@ int lcb_light_curve_elements(lcb_ctx* C, const lcb_model* model, const lcb_datum
         if (!P.model_ok[0]) throw Error(LCB_ERR_MODEL, P.model_err[0]);
         upload_plan(C, C->scratch, P, data, 0, true);
         DeviceSet& D = C->scratch;
-        const void* src[5] = {rec_dev, pos_dev, p64_dev, d64_dev, ecl_dev};
-        void* dst[5] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p, D.ecl.p};
-        for (int k = 0; k < 5; ++k)
+        const void* src[4] = {rec_dev, pos_dev, p64_dev, d64_dev};
+        void* dst[4] = {D.rec.p, D.pos.p, D.p64.p, D.d64.p};
+        for (int k = 0; k < 4; ++k)
             if (P.nelem)
                 CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], P.nelem * kElemBytes[k], cudaMemcpyDeviceToDevice, C->stream));
+        CUDA_TRY(cudaMemsetAsync(D.egrp.p, 0, ecl_groups(P) * sizeof(unsigned), C->stream));
+        CUDA_TRY(lcb::launch_ecl_import((const double2*)ecl_dev, P.nelem, D.ecl.as<double2>(), D.egrp.as<unsigned>(),
+                                        C->stream));
         enqueue_run(C, D, P, scale, rdata, false, kStageRest);
         std::vector<double> res, calc;
         std::vector<int> status;
@@ -1056,6 +1063,7 @@ size_t noalloc_carve(const lcb::Plan& P, unsigned char* base, DeviceSet& D) {
     take(D.p64, P.nelem * sizeof(double4));
     take(D.d64, P.nelem * sizeof(double4));
     take(D.ecl, P.nelem * lcb::kMaxEcl * sizeof(double2));
+    take(D.egrp, ecl_groups(P) * sizeof(unsigned));
     take(D.aux, nm * lcb::kNumAux * sizeof(double));
     take(D.status, nm * sizeof(int));
     take(D.spe, P.nsub * sizeof(float4));

@@ -16,6 +16,10 @@
 namespace lcb {
 
 constexpr int kMaxEcl = 4;        // eclipse pairs per element (star: 1 + 2 disc; disc: 2 + 2 stars)
+// The eclipse pairs are stored slot-major (pair k of element e at k * nelem + e), and a
+// word per group of kEclGroup consecutive elements records which slots any of them uses,
+// so the flux kernel stages only the slots a chunk of elements has.
+constexpr int kEclGroup = 64;
 constexpr int kMaxSpec = 9;       // special phases: 4 star1 ginterp + 4 star2 ginterp + wdwarf
 constexpr int kNumAux = 32;       // FP64 per-model accumulators
 

@@ -809,8 +809,12 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
     A.el_pos[e] = make_float4((float)px, (float)py, (float)pz, 0.f);
     A.el_p64[e] = make_double4(px, py, pz, (double)area);
     A.el_d64[e] = make_double4(dx, dy, dz, (double)grav);
-    double2* ep = A.el_ecl + e * kMaxEcl;
-    for (int k = 0; k < kMaxEcl; ++k) ep[k] = ecl[k];
+    unsigned used = 0;
+    for (int k = 0; k < kMaxEcl; ++k) {
+        A.el_ecl[k * A.sz.nelem + e] = ecl[k];
+        if (ecl[k].x <= 2.0) used |= 1u << k;
+    }
+    if (used) atomicOr(A.ecl_grp + e / kEclGroup, used);
 }
 
 // ---------------------------------------------------------------------------
@@ -831,8 +835,11 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs
         const int64_t e = sg.first + i;
         const double4 p = A.el_p64[e];
         double a, b;
-        if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt))
-            A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, by)] = make_double2(a, b);
+        if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt)) {
+            const int slot = roche_slot(sg.kind, by);
+            A.el_ecl[slot * A.sz.nelem + e] = make_double2(a, b);
+            atomicOr(A.ecl_grp + e / kEclGroup, 1u << slot);
+        }
         if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
     }
     roche_counters(A, cnt);
@@ -928,8 +935,11 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(El
     const bool found_eg = __shfl_xor_sync(0xffffffffu, (int)found, 1) != 0;
     const bool capped_eg = __shfl_xor_sync(0xffffffffu, (int)capped, 1) != 0;
     if (valid && part == 0) {
-        if (found && found_eg) A.el_ecl[e * kMaxEcl + roche_slot(sg.kind, blk.by)] =
-            make_double2(a, egress < a ? egress + 1.0 : egress);
+        if (found && found_eg) {
+            const int slot = roche_slot(sg.kind, blk.by);
+            A.el_ecl[slot * A.sz.nelem + e] = make_double2(a, egress < a ? egress + 1.0 : egress);
+            atomicOr(A.ecl_grp + e / kEclGroup, 1u << slot);
+        }
         if (capped || capped_eg) atomicOr(A.status + sg.model, kStatusIterCap);
     }
     roche_counters(A, cnt);
@@ -954,7 +964,7 @@ __global__ void __launch_bounds__(kElemThreads) k_aux(ElemArgs A) {
         px = p.x; py = p.y; pz = p.z; area = p.w;
         dx = d.x; dy = d.y; dz = d.z; grav = d.w;
         flux = (double)A.el_rec[e].w;
-        for (int k = 0; k < kMaxEcl; ++k) ecl[k] = A.el_ecl[e * kMaxEcl + k];
+        for (int k = 0; k < kMaxEcl; ++k) ecl[k] = A.el_ecl[k * A.sz.nelem + e];
     }
     double vals[16];
     int slot[16];
@@ -1117,7 +1127,8 @@ enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
 
 struct FluxSmem {
     float4 rec[2][kFluxChunk];
-    double2 ecl[2][kFluxChunk * kMaxEcl];
+    double2 ecl[2][kMaxEcl][kFluxChunk];  // the slots the chunk uses, slot-major
+    unsigned cmask[2];                    // which slots were staged
     uint16_t list[kFluxChunk];   // contributing elements of the chunk: index | (partly eclipsed << 15)
     int wtot[2][kFluxThreads / 32];
     uint64_t bar[2];
@@ -1134,22 +1145,18 @@ __device__ __forceinline__ int pair_cls(double ing, double eg, double lo, double
     return CLS_MIX;
 }
 
-// Moves the used pairs of one element to the front (empty pairs anywhere in
-// the slots) and classifies the element against the tile's phase range.
-__device__ __forceinline__ int classify(double2* e, const double* rlo, const double* rhi) {
-    int n = 0;
-    for (int k = 0; k < kMaxEcl; ++k) {
-        double2 p = e[k];
-        if (p.x <= 2.0) e[n++] = p;
-    }
-    for (int k = n; k < kMaxEcl; ++k) e[k] = make_double2(INFINITY, -INFINITY);
+// Classifies element e of a staged chunk against the tile's phase range from
+// the chunk's staged slots `cm` (an unused slot, (inf, -inf), is neutral).
+__device__ __forceinline__ int classify(const double2 (*ecl)[kFluxChunk], unsigned cm, int e, const double* rlo,
+                                        const double* rhi) {
     int res = -1;
     for (int h = 0; h < 2; ++h) {
         if (!(rlo[h] <= rhi[h])) continue;  // empty half
         int c = CLS_VIS;
-        for (int k = 0; k < n; ++k) {
-            double2 p = e[k];
-            int pc = pair_cls(p.x, p.y, rlo[h], rhi[h]);
+        for (int k = 0; k < kMaxEcl; ++k) {
+            if (!((cm >> k) & 1u)) continue;
+            const double2 p = ecl[k][e];
+            const int pc = pair_cls(p.x, p.y, rlo[h], rhi[h]);
             if (pc == CLS_HID) { c = CLS_HID; break; }
             if (pc == CLS_MIX) c = CLS_MIX;
         }
@@ -1181,11 +1188,11 @@ __device__ __forceinline__ float max_mu(const Arcs& a, float si, float ci, float
 }
 constexpr float kFacingMargin = 2e-5f;  // far above the FP32 rounding of mu
 
-__device__ __forceinline__ bool hidden_at(const double2* e, double phi) {
+__device__ __forceinline__ bool hidden_at(const double2 (*ecl)[kFluxChunk], unsigned cm, int e, double phi) {
     bool h = false;
     for (int k = 0; k < kMaxEcl; ++k) {
-        double2 p = e[k];
-        if (!(p.x <= 2.0)) break;
+        if (!((cm >> k) & 1u)) continue;
+        const double2 p = ecl[k][e];
         h |= (phi >= p.x && phi <= p.y) || phi <= p.y - 1.0;
     }
     return h;
@@ -1358,11 +1365,16 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         int b = c & 1;
         int64_t e0 = U.e0 + (int64_t)c * kFluxChunk;
         int n = min(kFluxChunk, U.ne - c * kFluxChunk);
-        uint32_t bytes = (uint32_t)n * (16u + 16u * kMaxEcl);
+        // only the eclipse slots some element of the chunk uses
+        unsigned cm = 0;
+        for (int64_t g = e0 / kEclGroup; g <= (e0 + n - 1) / kEclGroup; ++g) cm |= A.ecl_grp[g];
+        S.cmask[b] = cm;  // published to the waiting threads by the arrive below
+        uint32_t bytes = (uint32_t)n * 16u * (1u + (uint32_t)__popc(cm));
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect(&S.bar[b], bytes);
         bulk_load(S.rec[b], A.el_rec + e0, (uint32_t)n * 16u, &S.bar[b]);
-        bulk_load(S.ecl[b], A.el_ecl + e0 * kMaxEcl, (uint32_t)n * 16u * kMaxEcl, &S.bar[b]);
+        for (int k = 0; k < kMaxEcl; ++k)
+            if ((cm >> k) & 1u) bulk_load(S.ecl[b][k], A.el_ecl + k * A.sz.nelem + e0, (uint32_t)n * 16u, &S.bar[b]);
     };
     if (tid == 0) {
         if (nchunks > 0) issue(0);
@@ -1373,6 +1385,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         const int n = min(kFluxChunk, U.ne - c * kFluxChunk);
         if (!mbar_wait(&S.bar[b], parity[b])) atomicOr(A.status + U.model, kStatusTmaTimeout);
         parity[b] ^= 1u;
+        const unsigned cm = S.cmask[b];
         // classify every element of the chunk and list the contributing ones in
         // ascending order (ballot prefix sums): the loop below then runs over a
         // dense list without per-element branches
@@ -1384,7 +1397,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
             const int e = tid + rr * kFluxThreads;
             int cl = CLS_HID;
             if (e < n) {
-                cl = classify(&S.ecl[b][e * kMaxEcl], rlo, rhi);
+                cl = classify(S.ecl[b], cm, e, rlo, rhi);
                 if (cl != CLS_HID) {  // never facing the observer on this tile: contributes exactly 0
                     const float4 r = S.rec[b][e];
                     if (max_mu(arcs, sif, cif, r.x, r.y, r.z) <= face_thr) cl = CLS_HID;
@@ -1431,7 +1444,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll
                     for (int k = 0; k < kFluxR; ++k) {
                         float mu = ex[k] * r.x + ey[k] * r.y + ez[k] * r.z;
-                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(&S.ecl[b][e * kMaxEcl], ph[k]));
+                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k]));
                         if (v) {
                             float mag = 1.f;
                             if (lens) {
@@ -1456,13 +1469,12 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                 } else {
                     // sub-phases in pairs on the packed FP32x2 pipe
                     const float2 rx = make_float2(r.x, r.x), ry = make_float2(r.y, r.y), rz = make_float2(r.z, r.z);
-                    const double2* ee = &S.ecl[b][e * kMaxEcl];
 #pragma unroll
                     for (int k = 0; k < kFluxR; k += 2) {
                         const float2 mu = __ffma2_rn(ez2[k / 2], rz, __ffma2_rn(ey2[k / 2], ry, __fmul2_rn(ex2[k / 2], rx)));
                         const float2 c = C.pair(mu, r.w);
-                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(ee, ph[k]))) part[k] += c.x;
-                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(ee, ph[k + 1]))) part[k + 1] += c.y;
+                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k]))) part[k] += c.x;
+                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k + 1]))) part[k + 1] += c.y;
                     }
                 }
             }
@@ -1859,6 +1871,39 @@ cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflo
     cudaFree(out);
     *tflops = best;
     return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+__global__ void k_ecl_export(const double2* __restrict__ ecl, int64_t nelem, int64_t first, int64_t count,
+                             double2* __restrict__ out) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // (element, slot), slot fastest
+    if (j >= count * kMaxEcl) return;
+    const int64_t i = j / kMaxEcl;
+    const int k = (int)(j - i * kMaxEcl);
+    out[j] = ecl[k * nelem + first + i];
+}
+
+__global__ void k_ecl_import(const double2* __restrict__ in, int64_t nelem, double2* __restrict__ ecl,
+                             unsigned* __restrict__ grp) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nelem * kMaxEcl) return;
+    const int64_t e = j / kMaxEcl;
+    const int k = (int)(j - e * kMaxEcl);
+    const double2 p = in[j];
+    ecl[k * nelem + e] = p;
+    if (p.x <= 2.0) atomicOr(grp + e / kEclGroup, 1u << k);
+}
+
+cudaError_t launch_ecl_export(const double2* ecl, int64_t nelem, int64_t first, int64_t count, double2* out,
+                              cudaStream_t s) {
+    const int64_t n = count * kMaxEcl;
+    if (n > 0) k_ecl_export<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ecl, nelem, first, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ecl_import(const double2* in, int64_t nelem, double2* ecl, unsigned* ecl_grp, cudaStream_t s) {
+    const int64_t n = nelem * kMaxEcl;
+    if (n > 0) k_ecl_import<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, nelem, ecl, ecl_grp);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wait_probe(long long limit, int* status, long long* waited, cudaStream_t s) {

@@ -25,7 +25,8 @@ struct ElemArgs {
     float4* el_pos;      // posn.xyz, 0
     double4* el_p64;     // posn.xyz, area (FP64)
     double4* el_d64;     // dirn.xyz, gravity (FP64)
-    double2* el_ecl;     // 4 (ingress, egress) pairs per element
+    double2* el_ecl;     // kMaxEcl (ingress, egress) slots, slot-major: slot k of element e at k * sz.nelem + e
+    unsigned* ecl_grp;   // per kEclGroup elements: bit k set if any of them uses slot k (zeroed before k_elements)
     double* aux;         // kNumAux per model
     int* status;         // per model
     int64_t nblocks, nrblocks, nablocks;
@@ -56,7 +57,8 @@ struct FluxArgs {
     int* counter;
     const float4* el_rec;
     const float4* el_pos;
-    const double2* el_ecl;
+    const double2* el_ecl;     // slot-major, as ElemArgs::el_ecl
+    const unsigned* ecl_grp;   // slots used per kEclGroup elements
     const float4* sp_e;
     const double* sp_phi;
     const int8_t* sp_type;
@@ -95,6 +97,13 @@ cudaError_t launch_flux(const FluxArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_epilogue(const EpiArgs& a, cudaStream_t s);
 int flux_blocks_per_sm();
 cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflops);
+// Eclipse slots of elements [first, first + count) between the engine's slot-major
+// array (stride nelem) and element-major records of kMaxEcl pairs (the exchange format of
+// lcb_model_elements); the import also records the slots used in ecl_grp, which must be
+// zeroed first.
+cudaError_t launch_ecl_export(const double2* ecl, int64_t nelem, int64_t first, int64_t count, double2* out,
+                              cudaStream_t s);
+cudaError_t launch_ecl_import(const double2* in, int64_t nelem, double2* ecl, unsigned* ecl_grp, cudaStream_t s);
 // One block waiting on an mbarrier that nothing completes, bounded by `limit` cycles.
 cudaError_t launch_wait_probe(long long limit, int* status, long long* waited, cudaStream_t s);
 
