@@ -207,9 +207,9 @@ int  lcb_batch_results(lcb_batch* b, double* chisq_out, double* calc_out, lcb_re
 int  lcb_batch_stats(const lcb_batch* b, int64_t* out8);
 /* Eclipse-search counters of the last run: [potential evaluations, gradient
  * evaluations, line-of-sight searches, miss-proof nodes (a potential and a
- * gradient evaluation each), searches proven to
- * miss by the bound and skipped].  The line-of-sight searches are
- * exactly the reference path's (eclipse.rs:123-197 calls). */
+ * gradient evaluation each), successful miss proofs (one line of sight, or one
+ * block of consecutive phase-scan steps proven together)].  The line-of-sight
+ * searches are exactly the reference path's (eclipse.rs:123-197 calls). */
 int  lcb_batch_search_counts(const lcb_batch* b, int64_t* out5);
 /* Launch-shape choices of a resident batch, for an autotuner (no reference
  * counterpart; the reference GPU crate launches one fixed shape, 256-thread

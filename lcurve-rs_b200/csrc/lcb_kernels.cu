@@ -67,6 +67,15 @@ constexpr double kEfac = 1.0000001;                               // grid.rs:396
 #endif
 constexpr int kRocheMinBlocks = LCB_ROCHE_MIN_BLOCKS;  // k_roche blocks per SM (128 threads): register budget
 constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per line of sight before the full search
+#ifndef LCB_TUBE_MAX
+#define LCB_TUBE_MAX 8
+#endif
+constexpr int kTubeMax = LCB_TUBE_MAX;  // scan steps per phase-block miss proof (1: single steps only)
+#ifndef LCB_TUBE_BUDGET
+#define LCB_TUBE_BUDGET 24
+#endif
+constexpr int kTubeBudget = LCB_TUBE_BUDGET;  // nodes of one phase-block proof
+constexpr int kTubeCool = 8;  // single steps after a failed two-step block before the next block
 #ifndef LCB_CHOP_BUDGET
 #define LCB_CHOP_BUDGET 0
 #endif
@@ -232,8 +241,10 @@ __device__ __forceinline__ void closest_sq(const Los& L, double a, double b, dou
 }
 
 // The potential and its derivative along the line of sight at one point
-// (los_pot and los_dpot sharing the two distances).
-__device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, double lam, double& f, double& df) {
+// (los_pot and los_dpot sharing the two distances), and the gradient's norm
+// when `grad` is not null.
+__device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, double lam, double& f, double& df,
+                                             double* grad = nullptr) {
     double x = fma(lam, L.ex, L.px), y = fma(lam, L.ey, L.py), z = fma(lam, L.ez, L.pz);
     double x2y2 = x * x + y * y;
     double r1sq = x2y2 + z * z, r2sq = r1sq + 1.0 - 2.0 * x;
@@ -245,6 +256,7 @@ __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, do
     double gy = comp * y + mu1 * y - s.ssq * y;
     double gz = comp * z + mu1 * z;
     df = gx * L.ex + gy * L.ey + gz * L.ez;
+    if (grad) *grad = sqrt(gx * gx + gy * gy + gz * gz);
 }
 
 // True when the potential provably stays above the surface value on the whole
@@ -259,21 +271,44 @@ __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, do
 //   phi >= phi(m) - |phi'(m)| h / 2 - M h^2 / 8.
 // The bound must clear the surface value by 1e-9 relative (far above the
 // rounding of any evaluation).  False means "not proven".
-__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int budget, int& nodes) {
+//
+// With w > 0 the segment stands for a fan of lines through p whose unit
+// directions lie within w of L's: every point of the fan at parameter t is
+// within |t| w of L's point at t.  The Hessian of the potential has norm at
+// most H = 2 comp / r1^3 + 2 mu / r2^3 + ssq with r1, r2 now the closest
+// approaches of that tube, so a point x within r of the sub-segment's point y
+// has phi(x) >= phi(y) - |grad phi(y)| r - H r^2 / 2, and
+// |grad phi(y)| <= |grad phi(m)| + H h / 2: each node subtracts
+// (|grad phi(m)| + H h / 2) r + H r^2 / 2, r = (|m| + h / 2) w.
+__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int budget, int& nodes,
+                             double w = 0.0) {
     const double thr = s.pref + 1e-9 * fmax(fabs(s.pref), 1.0);
     const double hmin = 1e-6 * (b - a);
     double d1, d2;
     closest_sq(L, a, b, d1, d2);
     const double i1 = rsqrt(d1), i2 = rsqrt(d2);
     const double curv = 2.0 * s.comp * (i1 * i1 * i1) + 2.0 * s.mu * (i2 * i2 * i2) + s.ssq;
+    double hess = 0.0;
+    if (w > 0.0) {
+        const double widen = fmax(fabs(a), fabs(b)) * w;
+        const double r1 = sqrt(d1) - widen, r2 = sqrt(d2) - widen;
+        if (!(r1 > 1e-3 && r2 > 1e-3)) return false;
+        hess = 2.0 * s.comp / (r1 * r1 * r1) + 2.0 * s.mu / (r2 * r2 * r2) + s.ssq;
+    }
     double t = a, h = b - a;
     for (int it = 0; it < budget; ++it) {
         if (t >= b) return true;
         double hh = fmin(h, b - t);
         ++nodes;
-        double f, df;
-        los_pot_dpot(s, L, t + 0.5 * hh, f, df);
-        if (f - fabs(df) * (0.5 * hh) - curv * (0.125 * hh * hh) > thr) {
+        const double m = t + 0.5 * hh;
+        double f, df, g = 0.0;
+        los_pot_dpot(s, L, m, f, df, w > 0.0 ? &g : nullptr);
+        double bound = f - fabs(df) * (0.5 * hh) - curv * (0.125 * hh * hh);
+        if (w > 0.0) {
+            const double r = (fabs(m) + 0.5 * hh) * w;
+            bound -= (g + hess * (0.5 * hh)) * r + 0.5 * hess * r * r;
+        }
+        if (bound > thr) {
             t += hh;
             h = 2.0 * hh;
         } else {
@@ -292,29 +327,56 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
 // Not inlined: as a call, the search's working set does not add to the
 // registers the surrounding scan/bisection loop keeps live, which lets the
 // kernel run 5 blocks per SM (451 -> 350 ms on the 1024-model batch).
-__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, int prove) {
-    ++cnt.fbl;
+//
+// With tube_w > 0 the call is a phase-block miss proof instead: L is the middle
+// line of a block of scan steps whose directions lie within tube_w of L's, and
+// the result is true when every step of the block provably misses (each step's
+// own search would return false; see certify_miss).
+__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, int prove,
+                                    double tube_w = 0.0) {
     double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
-    double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
-    if (bq >= 0.0) return false;
-    double cq = (dx * dx + dy * dy + dz * dz) - sq(s.rref);
-    double fac = sq(bq) - cq;
-    if (fac <= 0.0) return false;
-    fac = sqrt(fac);
-    double lam2 = -bq + fac, lam1 = fmax(cq / lam2, 0.0);
-    if (lam1 == 0.0) return true;
-    const double pref = s.pref;
-    double step = lam2 - lam1;
-    if (!(step > acc)) return false;  // no evaluation: flam = 1 > f1 = f2 = 0
-    // the reference's first evaluation, at the middle of the chord
-    const double lam0 = lam1 + step / 2.0;
-    double flam = los_pot(s, L, lam0);
-    ++cnt.pot;
-    if (flam <= pref) return true;
-    if (prove > 0) {  // prove: the miss-proof node budget (0: no proof)
-        const double pad = 1.001 * acc + 1e-12;
-        if (certify_miss(s, L, lam1 - pad, lam2 + pad, prove, cnt.cert)) { ++cnt.skipped; return false; }
+    const double pad = 1.001 * acc + 1e-12;
+    double lam1, lam2, lam0 = 0.0;
+    if (tube_w > 0.0) {
+        // every step's b = e.d lies within |d| tube_w of the middle line's; its chord of the
+        // bounding sphere, where it has one, within [c / lam2max, lam2max] (lam2 = -b +
+        // sqrt(b^2 - c) falls as b rises)
+        const double dd = dx * dx + dy * dy + dz * dz;
+        const double cq = dd - sq(s.rref);
+        if (!(cq > 0.0)) return false;
+        const double bmin = L.ex * dx + L.ey * dy + L.ez * dz - sqrt(dd) * tube_w;
+        if (bmin >= 0.0) return true;  // every step: b >= 0, no chord
+        const double fac = sq(bmin) - cq;
+        if (fac <= 0.0) return true;   // every step misses the bounding sphere
+        lam2 = -bmin + sqrt(fac);
+        lam1 = cq / lam2;
+    } else {
+        ++cnt.fbl;
+        double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
+        if (bq >= 0.0) return false;
+        double cq = (dx * dx + dy * dy + dz * dz) - sq(s.rref);
+        double fac = sq(bq) - cq;
+        if (fac <= 0.0) return false;
+        fac = sqrt(fac);
+        lam2 = -bq + fac;
+        lam1 = fmax(cq / lam2, 0.0);
+        if (lam1 == 0.0) return true;
+        if (!(lam2 - lam1 > acc)) return false;  // no evaluation: flam = 1 > f1 = f2 = 0
+        // the reference's first evaluation, at the middle of the chord
+        lam0 = lam1 + (lam2 - lam1) / 2.0;
+        double flam = los_pot(s, L, lam0);
+        ++cnt.pot;
+        if (flam <= s.pref) return true;
     }
+    // one proof call site for both kinds of call (lanes of a warp reconverge in it)
+    if (prove > 0 && certify_miss(s, L, lam1 - pad, lam2 + pad, prove, cnt.cert, tube_w)) {
+        if (tube_w > 0.0) return true;
+        ++cnt.skipped;
+        return false;
+    }
+    if (tube_w > 0.0) return false;
+    const double pref = s.pref;
+    double step = lam2 - lam1, flam = los_pot(s, L, lam0);
     int nstep = 1;
     double f1 = los_pot(s, L, lam1), f2 = los_pot(s, L, lam2), lam = lam0;
     int local = 2;
@@ -399,6 +461,12 @@ __device__ __forceinline__ bool scan_setup(const RocheEcl& s, double cosi, doubl
     return true;
 }
 
+// Bound on |e(ph) - e(mid)| for phases within `half` of mid: the earth vector's
+// xy part (length sini) turns by 2 pi (ph - mid), a chord of 2 sini sin(pi |ph - mid|).
+__device__ __forceinline__ double tube_width(double sini, double half) {
+    return 2.0 * sini * sin(fmin(kPi * half, 0.5 * kPi)) * (1.0 + 1e-12) + 1e-15;
+}
+
 constexpr int kNoHit = 0x7f7f7f7f;  // first-hit sentinel (the byte pattern a memset of 0x7f writes)
 
 // `known_hit` >= 0: the scan's first hit is already known (split scan): go
@@ -406,6 +474,8 @@ constexpr int kNoHit = 0x7f7f7f7f;  // first-hit sentinel (the byte pattern a me
 // `only` = 1 or 2 runs just the ingress or just the egress bisection (the two are
 // independent: both start from the first hit), leaving `ing` resp. the unwrapped
 // `eg` set; the caller then applies egress < ingress -> egress + 1 itself.
+// kScan = false compiles the bisections alone (a known first hit is then required).
+template <bool kScan>
 __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, double delta, double px, double py,
                                double pz, double& ing, double& eg, bool& capped, EclCount& evals, int known_hit = -1,
                                int only = 0) {
@@ -416,7 +486,9 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
     const int nsteps = sc.nsteps;
     Los L{px, py, pz, 0.0, 0.0, 0.0};
     enum { SCAN, CHOP_IN, CHOP_EG };
-    int mode = SCAN, i = 0, it = 0;
+    // blk: scan steps the next phase-block proof covers; after a failed two-step block,
+    // kTubeCool single steps before the next (wait)
+    int mode = SCAN, i = 0, it = 0, blk = kTubeMax, wait = 0, last = 0;
     double phi = 0.0, pin = 0.0, pout = 0.0;
     if (known_hit >= 0) {  // as the scan below sets up its first hit
         phi = phi1 + (double)known_hit * dphi;
@@ -424,10 +496,16 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
         else { mode = CHOP_IN; pin = phi; pout = phi1; }
     }
     for (;;) {
-        double ph;
-        if (mode == SCAN) {
+        double ph, tube = 0.0;
+        if (kScan && mode == SCAN) {
             if (i > nsteps) return false;  // no eclipsed phase found
-            ph = phi1 + (double)i * dphi;
+            last = wait > 0 ? i : min(i + blk - 1, nsteps);
+            if (last > i) {  // steps i .. last at once: one phase-block proof
+                ph = phi1 + 0.5 * (double)(i + last) * dphi;
+                tube = tube_width(sini, 0.5 * (double)(last - i) * dphi);
+            } else {
+                ph = phi1 + (double)i * dphi;
+            }
         } else {
             if (!(fabs(pin - pout) > delta) || it >= 200) {
                 double r = (pin + pout) / 2.0;
@@ -446,11 +524,26 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
             ph = (pin + pout) / 2.0;
         }
         earth_at(cosi, sini, ph, L.ex, L.ey, L.ez);
-        const bool hit = fblink(s, acc, L, evals, capped, mode == SCAN ? kCertBudget : kChopBudget);
+        const bool hit = fblink(s, acc, L, evals, capped,
+                                !(kScan && mode == SCAN) ? kChopBudget : (tube > 0.0 ? kTubeBudget : kCertBudget), tube);
         if (capped) return false;
-        if (mode == SCAN) {
-            if (hit) { phi = ph; mode = CHOP_IN; pin = phi; pout = phi1; it = 0; }
-            else ++i;
+        if (kScan && mode == SCAN) {
+            if (tube > 0.0) {
+                if (hit) {  // the block's steps are all misses: counted as the searches they stand for
+                    evals.fbl += last - i + 1;
+                    ++evals.skipped;  // one proof
+                    i = last + 1;
+                    blk = min(2 * blk, kTubeMax);
+                } else {
+                    blk >>= 1;
+                    if (blk < 2) wait = kTubeCool;
+                }
+            } else if (hit) { phi = ph; mode = CHOP_IN; pin = phi; pout = phi1; it = 0; }
+            else {
+                ++i;
+                if (wait > 0) --wait;
+                if (wait == 0) blk = max(blk, min(2, kTubeMax));
+            }
         } else {
             if (hit) pin = ph; else pout = ph;
             ++it;
@@ -822,6 +915,22 @@ __global__ void __launch_bounds__(kElemThreads) k_elements(ElemArgs A) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void roche_counters(const ElemArgs& A, const EclCount& cnt);
 
+// ORs each lane's slot bits into its element group's used-slot word with one
+// atomic per distinct word of the warp (lanes hold consecutive elements, so a
+// warp spans one or two words).  All 32 lanes call it; g < 0 or bits == 0: none.
+__device__ __forceinline__ void group_or_warp(unsigned* grp, int64_t g, unsigned bits) {
+    const bool mine = bits != 0u && g >= 0;
+    unsigned pending = __ballot_sync(0xffffffffu, mine);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        const int64_t gs = __shfl_sync(0xffffffffu, g, src);
+        const bool same = mine && g == gs;
+        const unsigned all = __reduce_or_sync(0xffffffffu, same ? bits : 0u);
+        if ((int)(threadIdx.x & 31) == src) atomicOr(grp + gs, all);
+        pending &= ~__ballot_sync(0xffffffffu, same);
+    }
+}
+
 __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs A) {
     const ElemBlock blk = A.rblocks[blockIdx.x];
     const SegDesc sg = A.segs[blk.seg];
@@ -829,19 +938,23 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche(ElemArgs
     EclCount cnt;
     cnt.cap = A.fblink_cap;
     bool capped = false;
+    int64_t g = -1;
+    unsigned bits = 0u;
     if (i < sg.count && LCB_IN_BOUNDS(sg.first + i < A.sz.nelem, A.status + sg.model)) {
         const ModelDev& M = A.models[sg.model];
         const int by = blk.by;
         const int64_t e = sg.first + i;
         const double4 p = A.el_p64[e];
         double a, b;
-        if (ingress_egress(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt)) {
+        if (ingress_egress<true>(by == 1 ? M.ecl1 : M.ecl2, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt)) {
             const int slot = roche_slot(sg.kind, by);
             A.el_ecl[slot * A.sz.nelem + e] = make_double2(a, b);
-            atomicOr(A.ecl_grp + e / kEclGroup, 1u << slot);
+            g = e / kEclGroup;
+            bits = 1u << slot;
         }
         if (capped) atomicOr(A.status + sg.model, kStatusIterCap);
     }
+    group_or_warp(A.ecl_grp, g, bits);
     roche_counters(A, cnt);
 }
 
@@ -856,15 +969,32 @@ __device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double d
     const int total = sc.nsteps + 1, len = (total + split - 1) / split;
     const int lo = chunk * len, hi = min(total, lo + len);
     Los L{px, py, pz, 0.0, 0.0, 0.0};
-    for (int i = lo; i < hi; ++i) {
-        if (((i - lo) & 7) == 0 && *(volatile int*)first < lo) return;
-        earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
-        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget);
+    int blk = kTubeMax, wait = 0, n = 0;  // phase blocks as in ingress_egress
+    for (int i = lo; i < hi; ++n) {
+        if ((n & 7) == 0 && *(volatile int*)first < lo) return;
+        const int last = wait > 0 ? i : min(i + blk - 1, hi - 1);
+        const double tube = last > i ? tube_width(sini, 0.5 * (double)(last - i) * sc.dphi) : 0.0;
+        earth_at(cosi, sini, sc.phi1 + 0.5 * (double)(i + last) * sc.dphi, L.ex, L.ey, L.ez);
+        const bool r = fblink(s, sc.acc, L, evals, capped, tube > 0.0 ? kTubeBudget : kCertBudget, tube);
         if (capped) return;
-        if (hit) {
+        if (tube > 0.0) {
+            if (r) {
+                ++evals.skipped;  // one proof
+                i = last + 1;
+                blk = min(2 * blk, kTubeMax);
+            } else {
+                blk >>= 1;
+                if (blk < 2) wait = kTubeCool;
+            }
+            continue;
+        }
+        if (r) {
             atomicMin(first, i);
             return;
         }
+        ++i;
+        if (wait > 0) --wait;
+        if (wait == 0) blk = max(blk, min(2, kTubeMax));
     }
 }
 
@@ -929,19 +1059,23 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(El
         Scan sc;
         if (part == 0 && scan_setup(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, sc))
             cnt.fbl += first == kNoHit ? sc.nsteps + 1 : first + 1;  // the single scan's searches
-        found = ingress_egress(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt, first, part + 1);
+        found = ingress_egress<false>(R, M.cosi_e, M.sini_e, M.delta, p.x, p.y, p.z, a, b, capped, cnt, first, part + 1);
     }
     const double egress = __shfl_xor_sync(0xffffffffu, b, 1);
     const bool found_eg = __shfl_xor_sync(0xffffffffu, (int)found, 1) != 0;
     const bool capped_eg = __shfl_xor_sync(0xffffffffu, (int)capped, 1) != 0;
+    int64_t g = -1;
+    unsigned bits = 0u;
     if (valid && part == 0) {
         if (found && found_eg) {
             const int slot = roche_slot(sg.kind, blk.by);
             A.el_ecl[slot * A.sz.nelem + e] = make_double2(a, egress < a ? egress + 1.0 : egress);
-            atomicOr(A.ecl_grp + e / kEclGroup, 1u << slot);
+            g = e / kEclGroup;
+            bits = 1u << slot;
         }
         if (capped || capped_eg) atomicOr(A.status + sg.model, kStatusIterCap);
     }
+    group_or_warp(A.ecl_grp, g, bits);
     roche_counters(A, cnt);
 }
 
@@ -1124,11 +1258,14 @@ __global__ void k_wait_probe(long long limit, int* status, long long* waited) {
 }
 
 enum { CLS_VIS = 0, CLS_MIX = 1, CLS_HID = 2 };
+// used-slot words a flux unit spans (units hold at most 16 chunks of elements)
+constexpr int kUnitGroups = 16 * kFluxChunk / kEclGroup + 2;
 
 struct FluxSmem {
     float4 rec[2][kFluxChunk];
     double2 ecl[2][kMaxEcl][kFluxChunk];  // the slots the chunk uses, slot-major
     unsigned cmask[2];                    // which slots were staged
+    unsigned gw[kUnitGroups];             // the unit's words of used-slot masks (ecl_grp)
     uint16_t list[kFluxChunk];   // contributing elements of the chunk: index | (partly eclipsed << 15)
     int wtot[2][kFluxThreads / 32];
     uint64_t bar[2];
@@ -1309,6 +1446,10 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
             }
         }
     }
+    // the unit's used-slot words, read once (issue() combines them per chunk)
+    const int64_t g0 = U.e0 / kEclGroup;
+    const int ngw = (int)((U.e0 + U.ne - 1) / kEclGroup - g0 + 1);
+    for (int t = tid; t < ngw && t < kUnitGroups; t += kFluxThreads) S.gw[t] = A.ecl_grp[g0 + t];
     // block min/max of the two halves
     for (int h = 0; h < 2; ++h) {
         double a = dlo[h], b = dhi[h];
@@ -1367,7 +1508,8 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
         int n = min(kFluxChunk, U.ne - c * kFluxChunk);
         // only the eclipse slots some element of the chunk uses
         unsigned cm = 0;
-        for (int64_t g = e0 / kEclGroup; g <= (e0 + n - 1) / kEclGroup; ++g) cm |= A.ecl_grp[g];
+        for (int64_t g = e0 / kEclGroup; g <= (e0 + n - 1) / kEclGroup; ++g)
+            cm |= g - g0 < kUnitGroups ? S.gw[g - g0] : A.ecl_grp[g];
         S.cmask[b] = cm;  // published to the waiting threads by the arrive below
         uint32_t bytes = (uint32_t)n * 16u * (1u + (uint32_t)__popc(cm));
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
