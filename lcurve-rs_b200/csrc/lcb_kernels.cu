@@ -280,8 +280,9 @@ __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, do
 // has phi(x) >= phi(y) - |grad phi(y)| r - H r^2 / 2, and
 // |grad phi(y)| <= |grad phi(m)| + H h / 2: each node subtracts
 // (|grad phi(m)| + H h / 2) r + H r^2 / 2, r = (|m| + h / 2) w.
-__device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int budget, int& nodes,
-                             double w = 0.0) {
+template <bool kTube>
+__device__ __forceinline__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b, int budget,
+                                             int& nodes, double w = 0.0) {
     const double thr = s.pref + 1e-9 * fmax(fabs(s.pref), 1.0);
     const double hmin = 1e-6 * (b - a);
     double d1, d2;
@@ -289,7 +290,7 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
     const double i1 = rsqrt(d1), i2 = rsqrt(d2);
     const double curv = 2.0 * s.comp * (i1 * i1 * i1) + 2.0 * s.mu * (i2 * i2 * i2) + s.ssq;
     double hess = 0.0;
-    if (w > 0.0) {
+    if (kTube) {
         const double widen = fmax(fabs(a), fabs(b)) * w;
         const double r1 = sqrt(d1) - widen, r2 = sqrt(d2) - widen;
         if (!(r1 > 1e-3 && r2 > 1e-3)) return false;
@@ -302,9 +303,9 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
         ++nodes;
         const double m = t + 0.5 * hh;
         double f, df, g = 0.0;
-        los_pot_dpot(s, L, m, f, df, w > 0.0 ? &g : nullptr);
+        los_pot_dpot(s, L, m, f, df, kTube ? &g : nullptr);
         double bound = f - fabs(df) * (0.5 * hh) - curv * (0.125 * hh * hh);
-        if (w > 0.0) {
+        if (kTube) {
             const double r = (fabs(m) + 0.5 * hh) * w;
             bound -= (g + hess * (0.5 * hh)) * r + 0.5 * hess * r * r;
         }
@@ -327,56 +328,29 @@ __device__ bool certify_miss(const RocheEcl& s, const Los& L, double a, double b
 // Not inlined: as a call, the search's working set does not add to the
 // registers the surrounding scan/bisection loop keeps live, which lets the
 // kernel run 5 blocks per SM (451 -> 350 ms on the 1024-model batch).
-//
-// With tube_w > 0 the call is a phase-block miss proof instead: L is the middle
-// line of a block of scan steps whose directions lie within tube_w of L's, and
-// the result is true when every step of the block provably misses (each step's
-// own search would return false; see certify_miss).
-__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, int prove,
-                                    double tube_w = 0.0) {
+__device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L, EclCount& cnt, bool& capped, int prove) {
+    ++cnt.fbl;
     double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
-    const double pad = 1.001 * acc + 1e-12;
-    double lam1, lam2, lam0 = 0.0;
-    if (tube_w > 0.0) {
-        // every step's b = e.d lies within |d| tube_w of the middle line's; its chord of the
-        // bounding sphere, where it has one, within [c / lam2max, lam2max] (lam2 = -b +
-        // sqrt(b^2 - c) falls as b rises)
-        const double dd = dx * dx + dy * dy + dz * dz;
-        const double cq = dd - sq(s.rref);
-        if (!(cq > 0.0)) return false;
-        const double bmin = L.ex * dx + L.ey * dy + L.ez * dz - sqrt(dd) * tube_w;
-        if (bmin >= 0.0) return true;  // every step: b >= 0, no chord
-        const double fac = sq(bmin) - cq;
-        if (fac <= 0.0) return true;   // every step misses the bounding sphere
-        lam2 = -bmin + sqrt(fac);
-        lam1 = cq / lam2;
-    } else {
-        ++cnt.fbl;
-        double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
-        if (bq >= 0.0) return false;
-        double cq = (dx * dx + dy * dy + dz * dz) - sq(s.rref);
-        double fac = sq(bq) - cq;
-        if (fac <= 0.0) return false;
-        fac = sqrt(fac);
-        lam2 = -bq + fac;
-        lam1 = fmax(cq / lam2, 0.0);
-        if (lam1 == 0.0) return true;
-        if (!(lam2 - lam1 > acc)) return false;  // no evaluation: flam = 1 > f1 = f2 = 0
-        // the reference's first evaluation, at the middle of the chord
-        lam0 = lam1 + (lam2 - lam1) / 2.0;
-        double flam = los_pot(s, L, lam0);
-        ++cnt.pot;
-        if (flam <= s.pref) return true;
-    }
-    // one proof call site for both kinds of call (lanes of a warp reconverge in it)
-    if (prove > 0 && certify_miss(s, L, lam1 - pad, lam2 + pad, prove, cnt.cert, tube_w)) {
-        if (tube_w > 0.0) return true;
-        ++cnt.skipped;
-        return false;
-    }
-    if (tube_w > 0.0) return false;
+    double bq = L.ex * dx + L.ey * dy + L.ez * dz;  // sphere_eclipse_los, eclipse.rs:202-224
+    if (bq >= 0.0) return false;
+    double cq = (dx * dx + dy * dy + dz * dz) - sq(s.rref);
+    double fac = sq(bq) - cq;
+    if (fac <= 0.0) return false;
+    fac = sqrt(fac);
+    double lam2 = -bq + fac, lam1 = fmax(cq / lam2, 0.0);
+    if (lam1 == 0.0) return true;
     const double pref = s.pref;
-    double step = lam2 - lam1, flam = los_pot(s, L, lam0);
+    double step = lam2 - lam1;
+    if (!(step > acc)) return false;  // no evaluation: flam = 1 > f1 = f2 = 0
+    // the reference's first evaluation, at the middle of the chord
+    const double lam0 = lam1 + step / 2.0;
+    double flam = los_pot(s, L, lam0);
+    ++cnt.pot;
+    if (flam <= pref) return true;
+    if (prove > 0) {  // prove: the miss-proof node budget (0: no proof)
+        const double pad = 1.001 * acc + 1e-12;
+        if (certify_miss<false>(s, L, lam1 - pad, lam2 + pad, prove, cnt.cert)) { ++cnt.skipped; return false; }
+    }
     int nstep = 1;
     double f1 = los_pot(s, L, lam1), f2 = los_pot(s, L, lam2), lam = lam0;
     int local = 2;
@@ -401,6 +375,29 @@ __device__ __noinline__ bool fblink(const RocheEcl& s, double acc, const Los& L,
     cnt.pot += local;
     if (br) return dbrent_below(s, L, lam1, lam, lam2, acc, pref, cnt, local, capped);
     return false;
+}
+
+// Phase-block miss proof: L is the middle line of a block of consecutive scan
+// steps whose unit directions lie within tube_w of L's (all lines pass through
+// p).  True when every step of the block provably misses, i.e. each step's own
+// fblink would return false (see certify_miss).  A separate call from fblink:
+// the single-step search keeps its own, smaller register allocation.
+__device__ __noinline__ bool tube_miss(const RocheEcl& s, double acc, const Los& L, double tube_w, int budget,
+                                       int& nodes) {
+    const double dx = L.px - s.cofmx, dy = L.py, dz = L.pz;
+    // every step's b = e.d lies within |d| tube_w of the middle line's; its chord of the
+    // bounding sphere, where it has one, within [c / lam2max, lam2max] (lam2 = -b +
+    // sqrt(b^2 - c) falls as b rises)
+    const double dd = dx * dx + dy * dy + dz * dz;
+    const double cq = dd - sq(s.rref);
+    if (!(cq > 0.0)) return false;
+    const double bmin = L.ex * dx + L.ey * dy + L.ez * dz - sqrt(dd) * tube_w;
+    if (bmin >= 0.0) return true;  // every step: b >= 0, no chord
+    const double fac = sq(bmin) - cq;
+    if (fac <= 0.0) return true;   // every step misses the bounding sphere
+    const double lam2 = -bmin + sqrt(fac), lam1 = cq / lam2;
+    const double pad = 1.001 * acc + 1e-12;
+    return certify_miss<true>(s, L, lam1 - pad, lam2 + pad, budget, nodes, tube_w);
 }
 
 __device__ __forceinline__ void earth_at(double cosi, double sini, double phase, double& ex, double& ey, double& ez) {
@@ -524,8 +521,8 @@ __device__ bool ingress_egress(const RocheEcl& s, double cosi, double sini, doub
             ph = (pin + pout) / 2.0;
         }
         earth_at(cosi, sini, ph, L.ex, L.ey, L.ez);
-        const bool hit = fblink(s, acc, L, evals, capped,
-                                !(kScan && mode == SCAN) ? kChopBudget : (tube > 0.0 ? kTubeBudget : kCertBudget), tube);
+        const bool hit = tube > 0.0 ? tube_miss(s, acc, L, tube, kTubeBudget, evals.cert)
+                                    : fblink(s, acc, L, evals, capped, !(kScan && mode == SCAN) ? kChopBudget : kCertBudget);
         if (capped) return false;
         if (kScan && mode == SCAN) {
             if (tube > 0.0) {
@@ -969,32 +966,15 @@ __device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double d
     const int total = sc.nsteps + 1, len = (total + split - 1) / split;
     const int lo = chunk * len, hi = min(total, lo + len);
     Los L{px, py, pz, 0.0, 0.0, 0.0};
-    int blk = kTubeMax, wait = 0, n = 0;  // phase blocks as in ingress_egress
-    for (int i = lo; i < hi; ++n) {
-        if ((n & 7) == 0 && *(volatile int*)first < lo) return;
-        const int last = wait > 0 ? i : min(i + blk - 1, hi - 1);
-        const double tube = last > i ? tube_width(sini, 0.5 * (double)(last - i) * sc.dphi) : 0.0;
-        earth_at(cosi, sini, sc.phi1 + 0.5 * (double)(i + last) * sc.dphi, L.ex, L.ey, L.ez);
-        const bool r = fblink(s, sc.acc, L, evals, capped, tube > 0.0 ? kTubeBudget : kCertBudget, tube);
+    for (int i = lo; i < hi; ++i) {
+        if (((i - lo) & 7) == 0 && *(volatile int*)first < lo) return;
+        earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
+        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget);
         if (capped) return;
-        if (tube > 0.0) {
-            if (r) {
-                ++evals.skipped;  // one proof
-                i = last + 1;
-                blk = min(2 * blk, kTubeMax);
-            } else {
-                blk >>= 1;
-                if (blk < 2) wait = kTubeCool;
-            }
-            continue;
-        }
-        if (r) {
+        if (hit) {
             atomicMin(first, i);
             return;
         }
-        ++i;
-        if (wait > 0) --wait;
-        if (wait == 0) blk = max(blk, min(2, kTubeMax));
     }
 }
 
@@ -1290,9 +1270,8 @@ __device__ __forceinline__ int classify(const double2 (*ecl)[kFluxChunk], unsign
     for (int h = 0; h < 2; ++h) {
         if (!(rlo[h] <= rhi[h])) continue;  // empty half
         int c = CLS_VIS;
-        for (int k = 0; k < kMaxEcl; ++k) {
-            if (!((cm >> k) & 1u)) continue;
-            const double2 p = ecl[k][e];
+        for (unsigned m = cm; m; m &= m - 1u) {
+            const double2 p = ecl[__ffs(m) - 1][e];
             const int pc = pair_cls(p.x, p.y, rlo[h], rhi[h]);
             if (pc == CLS_HID) { c = CLS_HID; break; }
             if (pc == CLS_MIX) c = CLS_MIX;
@@ -1327,9 +1306,8 @@ constexpr float kFacingMargin = 2e-5f;  // far above the FP32 rounding of mu
 
 __device__ __forceinline__ bool hidden_at(const double2 (*ecl)[kFluxChunk], unsigned cm, int e, double phi) {
     bool h = false;
-    for (int k = 0; k < kMaxEcl; ++k) {
-        if (!((cm >> k) & 1u)) continue;
-        const double2 p = ecl[k][e];
+    for (unsigned m = cm; m; m &= m - 1u) {  // the staged slots only
+        const double2 p = ecl[__ffs(m) - 1][e];
         h |= (phi >= p.x && phi <= p.y) || phi <= p.y - 1.0;
     }
     return h;

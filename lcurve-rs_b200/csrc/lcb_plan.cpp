@@ -986,12 +986,16 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
                 for (int64_t off = 0; off < g.count; off += kRocheBlock) P.rblocks[k++] = ElemBlock{(int32_t)s, by, off};
     });
 
-    // small batches: spread each element's phase scan over several threads until
-    // about four waves of Roche blocks fill the GPU (large batches keep one)
+    // small batches: spread each element's phase scan over several threads, a power
+    // of two up to 16, until about sixteen waves of scan threads fill the GPU (the
+    // choices an autotuning of 8..128-model batches made; large batches keep one
+    // thread per element, where the scan proves blocks of steps at once)
     {
         const int64_t threads = (int64_t)P.rblocks.size() * kRocheBlock;
-        const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 4;
-        P.roche_split = threads > 0 ? (int)std::min<int64_t>(std::max<int64_t>(target / threads, 1), 16) : 1;
+        const int64_t target = (int64_t)std::max(num_sms, 1) * 640 * 16;
+        int split = 1;
+        while (threads > 0 && split < 16 && (int64_t)(2 * split) * threads <= target) split *= 2;
+        P.roche_split = split;
         if (tune.roche_split > 0 && threads > 0) P.roche_split = std::min(std::max(tune.roche_split, 1), 16);
     }
 
