@@ -1246,12 +1246,13 @@ struct FluxSmem {
     double2 ecl[2][kMaxEcl][kFluxChunk];  // the slots the chunk uses, slot-major
     unsigned cmask[2];                    // which slots were staged
     unsigned gw[kUnitGroups];             // the unit's words of used-slot masks (ecl_grp)
-    uint16_t list[kFluxChunk];   // contributing elements of the chunk: index | (partly eclipsed << 15)
+    uint16_t list[kFluxChunk];   // contributing elements: index | pairs << 8 | (partly eclipsed << 15)
     int wtot[2][kFluxThreads / 32];
     uint64_t bar[2];
     int unit;
 };
 static_assert(kFluxChunk == 2 * kFluxThreads, "the classification pass gives each thread two elements");
+static_assert(kFluxChunk <= 256 && kMaxEcl < 8, "list entries hold the element in 8 bits and its pairs in 3");
 
 size_t flux_smem_bytes_impl() { return sizeof(FluxSmem); }
 
@@ -1282,6 +1283,17 @@ __device__ __forceinline__ int classify(const double2 (*ecl)[kFluxChunk], unsign
     return res < 0 ? CLS_HID : res;
 }
 
+// Moves element e's used pairs among the staged slots `cm` to slots 0, 1, ..
+// (in place: a pair only moves to a lower slot); returns their number.
+__device__ __forceinline__ int compact_pairs(double2 (*ecl)[kFluxChunk], unsigned cm, int e) {
+    int n = 0;
+    for (unsigned m = cm; m; m &= m - 1u) {
+        const double2 p = ecl[__ffs(m) - 1][e];
+        if (p.x <= 2.0) ecl[n++][e] = p;
+    }
+    return n;
+}
+
 // The earth vector of phase theta/2pi is (sini cos t, -sini sin t, cosi), so an
 // element's mu over a phase arc is A cos t + B sin t + C.  The tile's active
 // sub-phases lie on (at most) two arcs shorter than pi, one per half of [0, 1).
@@ -1304,10 +1316,12 @@ __device__ __forceinline__ float max_mu(const Arcs& a, float si, float ci, float
 }
 constexpr float kFacingMargin = 2e-5f;  // far above the FP32 rounding of mu
 
-__device__ __forceinline__ bool hidden_at(const double2 (*ecl)[kFluxChunk], unsigned cm, int e, double phi) {
+// Is element e behind one of its npair pairs (moved to slots 0 .. npair-1 by
+// compact_pairs) at phase phi?
+__device__ __forceinline__ bool hidden_at(const double2 (*ecl)[kFluxChunk], int npair, int e, double phi) {
     bool h = false;
-    for (unsigned m = cm; m; m &= m - 1u) {  // the staged slots only
-        const double2 p = ecl[__ffs(m) - 1][e];
+    for (int k = 0; k < npair; ++k) {
+        const double2 p = ecl[k][e];
         h |= (phi >= p.x && phi <= p.y) || phi <= p.y - 1.0;
     }
     return h;
@@ -1523,7 +1537,9 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                     if (max_mu(arcs, sif, cif, r.x, r.y, r.z) <= face_thr) cl = CLS_HID;
                 }
             }
-            ent[rr] = (uint16_t)(e | (cl == CLS_MIX ? 0x8000 : 0));
+            // list entry: element | pairs << 8 | partly eclipsed << 15 (the pairs of a
+            // partly eclipsed element are moved to the front for hidden_at)
+            ent[rr] = (uint16_t)(cl == CLS_MIX ? (e | compact_pairs(S.ecl[b], cm, e) << 8 | 0x8000) : e);
             keep[rr] = __ballot_sync(0xffffffffu, cl != CLS_HID);
             if (lane == 0) S.wtot[rr][warp] = __popc(keep[rr]);
         }
@@ -1552,7 +1568,8 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll 4
             for (int q = s0; q < s1; ++q) {
                 const int ev = S.list[q];
-                const int e = ev & 0x7fff;
+                const int e = ev & 0xff;
+                const int npair = (ev >> 8) & 7;
                 const int cls = (ev & 0x8000) ? CLS_MIX : CLS_VIS;
                 const float4 r = S.rec[b][e];
                 if (KIND == UK_STAR_GENERIC) {
@@ -1564,7 +1581,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll
                     for (int k = 0; k < kFluxR; ++k) {
                         float mu = ex[k] * r.x + ey[k] * r.y + ez[k] * r.z;
-                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k]));
+                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k]));
                         if (v) {
                             float mag = 1.f;
                             if (lens) {
@@ -1593,8 +1610,8 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                     for (int k = 0; k < kFluxR; k += 2) {
                         const float2 mu = __ffma2_rn(ez2[k / 2], rz, __ffma2_rn(ey2[k / 2], ry, __fmul2_rn(ex2[k / 2], rx)));
                         const float2 c = C.pair(mu, r.w);
-                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k]))) part[k] += c.x;
-                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], cm, e, ph[k + 1]))) part[k + 1] += c.y;
+                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k]))) part[k] += c.x;
+                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k + 1]))) part[k + 1] += c.y;
                     }
                 }
             }
