@@ -1316,13 +1316,17 @@ __device__ __forceinline__ float max_mu(const Arcs& a, float si, float ci, float
 }
 constexpr float kFacingMargin = 2e-5f;  // far above the FP32 rounding of mu
 
-// Is element e behind one of its npair pairs (moved to slots 0 .. npair-1 by
-// compact_pairs) at phase phi?
-__device__ __forceinline__ bool hidden_at(const double2 (*ecl)[kFluxChunk], int npair, int e, double phi) {
-    bool h = false;
-    for (int k = 0; k < npair; ++k) {
-        const double2 p = ecl[k][e];
-        h |= (phi >= p.x && phi <= p.y) || phi <= p.y - 1.0;
+// The thread's sub-phases (bit k: phase ph[k]) at which element e is behind one
+// of its npair pairs (moved to slots 0 .. npair-1 by compact_pairs).
+__device__ __forceinline__ unsigned hidden_mask(const double2 (*ecl)[kFluxChunk], int npair, int e,
+                                                const double* ph) {
+    unsigned h = 0u;
+#pragma unroll 1
+    for (int j = 0; j < npair; ++j) {
+        const double2 p = ecl[j][e];
+#pragma unroll
+        for (int k = 0; k < kFluxR; ++k)
+            h |= (((ph[k] >= p.x && ph[k] <= p.y) || ph[k] <= p.y - 1.0) ? 1u : 0u) << k;
     }
     return h;
 }
@@ -1569,9 +1573,9 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
             for (int q = s0; q < s1; ++q) {
                 const int ev = S.list[q];
                 const int e = ev & 0xff;
-                const int npair = (ev >> 8) & 7;
-                const int cls = (ev & 0x8000) ? CLS_MIX : CLS_VIS;
                 const float4 r = S.rec[b][e];
+                // sub-phases behind one of a partly eclipsed element's pairs (bit k: sub-phase k)
+                const unsigned hid = (ev & 0x8000) ? hidden_mask(S.ecl[b], (ev >> 8) & 7, e, ph) : 0u;
                 if (KIND == UK_STAR_GENERIC) {
                     const float4 p = __ldg(A.el_pos + U.e0 + (int64_t)c * kFluxChunk + e);
                     float vx, vy;
@@ -1581,7 +1585,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll
                     for (int k = 0; k < kFluxR; ++k) {
                         float mu = ex[k] * r.x + ey[k] * r.y + ez[k] * r.z;
-                        bool v = mu > thrg && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k]));
+                        bool v = mu > thrg && !((hid >> k) & 1u);
                         if (v) {
                             float mag = 1.f;
                             if (lens) {
@@ -1610,8 +1614,8 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
                     for (int k = 0; k < kFluxR; k += 2) {
                         const float2 mu = __ffma2_rn(ez2[k / 2], rz, __ffma2_rn(ey2[k / 2], ry, __fmul2_rn(ex2[k / 2], rx)));
                         const float2 c = C.pair(mu, r.w);
-                        if (mu.x > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k]))) part[k] += c.x;
-                        if (mu.y > C.thr && (cls == CLS_VIS || !hidden_at(S.ecl[b], npair, e, ph[k + 1]))) part[k + 1] += c.y;
+                        if (mu.x > C.thr && !((hid >> k) & 1u)) part[k] += c.x;
+                        if (mu.y > C.thr && !((hid >> (k + 1)) & 1u)) part[k + 1] += c.y;
                     }
                 }
             }
