@@ -361,8 +361,10 @@ class Batch:
 
     def set_params(self, names, values) -> None:
         values = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(self.n, len(names)))
-        arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
-        check(_capi.load().lcb_batch_set_params(self._h, arr, len(names), dptr(values)))
+        key = tuple(names)
+        if getattr(self, "_names_key", None) != key:  # the C array of names, kept across calls
+            self._names_key, self._names_arr = key, (C.c_char_p * len(names))(*[n.encode() for n in names])
+        check(_capi.load().lcb_batch_set_params(self._h, self._names_arr, len(names), dptr(values)))
 
     def run(self, scale=False) -> None:
         check(_capi.load().lcb_batch_run(self._h, int(bool(scale))))

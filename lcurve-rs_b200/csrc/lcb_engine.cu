@@ -135,25 +135,37 @@ namespace {
 // Words of the per-group eclipse slot masks (one per kEclGroup elements).
 size_t ecl_groups(const lcb::Plan& P) { return (size_t)((P.nelem + lcb::kEclGroup - 1) / lcb::kEclGroup); }
 
+// `prev` (a resident batch's previous plan, its tables already on the device):
+// tables equal to prev's are not uploaded again (a re-parameterised batch of
+// unchanged shape usually changes only the model table and the grid bands).
 void upload_plan(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, const lcb_datum* data, int64_t ndata_src,
-                 bool upload_data) {
+                 bool upload_data, const lcb::Plan* prev = nullptr) {
     cudaStream_t s = C->stream;
     auto put = [&](DevBuf& b, const void* src, size_t bytes) {
         b.ensure(bytes);
         if (bytes) CUDA_TRY(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
         C->h2d += (int64_t)bytes;
     };
+    // a table equal to the previous plan's is already on the device
+    auto put_new = [&](DevBuf& b, const auto& now, const auto& before) {
+        const size_t bytes = now.size() * sizeof(now[0]);
+        if (prev && b.p && b.cap >= bytes && before.size() == now.size() &&
+            (bytes == 0 || std::memcmp(now.data(), before.data(), bytes) == 0))
+            return;
+        put(b, now.data(), bytes);
+    };
     const int64_t nm = (int64_t)P.models.size();
     put(D.models, P.models.data(), nm * sizeof(lcb::ModelDev));
-    put(D.segs, P.segs.data(), P.segs.size() * sizeof(lcb::SegDesc));
-    put(D.bands, P.bands.data(), P.bands.size() * sizeof(lcb::Band));
-    put(D.rings, P.rings.data(), P.rings.size() * sizeof(lcb::Ring));
-    put(D.eblocks, P.eblocks.data(), P.eblocks.size() * sizeof(lcb::ElemBlock));
-    put(D.rblocks, P.rblocks.data(), P.rblocks.size() * sizeof(lcb::ElemBlock));
-    put(D.ablocks, P.ablocks.data(), P.ablocks.size() * sizeof(lcb::ElemBlock));
-    put(D.units, P.units.data(), P.units.size() * sizeof(lcb::FluxUnit));
-    put(D.dmodel, P.datum_model.data(), P.datum_model.size() * sizeof(int32_t));
-    put(D.dsub0, P.datum_sub0.data(), P.datum_sub0.size() * sizeof(int64_t));
+    const lcb::Plan& Q = prev ? *prev : P;
+    put_new(D.segs, P.segs, Q.segs);
+    put_new(D.bands, P.bands, Q.bands);
+    put_new(D.rings, P.rings, Q.rings);
+    put_new(D.eblocks, P.eblocks, Q.eblocks);
+    put_new(D.rblocks, P.rblocks, Q.rblocks);
+    put_new(D.ablocks, P.ablocks, Q.ablocks);
+    put_new(D.units, P.units, Q.units);
+    put_new(D.dmodel, P.datum_model, Q.datum_model);
+    put_new(D.dsub0, P.datum_sub0, Q.datum_sub0);
     if (upload_data) {
         (void)ndata_src;
         if (P.datum_contiguous && P.ndatum > 0) {
@@ -256,7 +268,7 @@ void enqueue_run(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, int scale, int rd
 void set_device(lcb_ctx* C) { CUDA_TRY(cudaSetDevice(C->device)); }
 
 void fetch_results(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, std::vector<double>& res, std::vector<double>* calc,
-                   std::vector<int>* status) {
+                   std::vector<int>* status, unsigned long long* ecount = nullptr) {
     const int64_t nm = (int64_t)P.models.size();
     res.resize(nm * 12);
     CUDA_TRY(cudaMemcpyAsync(res.data(), D.results.p, nm * 12 * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
@@ -269,6 +281,8 @@ void fetch_results(lcb_ctx* C, DeviceSet& D, const lcb::Plan& P, std::vector<dou
         status->resize(nm);
         CUDA_TRY(cudaMemcpyAsync(status->data(), D.status.p, nm * sizeof(int), cudaMemcpyDeviceToHost, C->stream));
     }
+    if (ecount)  // the eclipse-search counters (5)
+        CUDA_TRY(cudaMemcpyAsync(ecount, D.ecount.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, C->stream));
     C->d2h += (int64_t)(nm * 12 * sizeof(double)) + (calc ? P.ndatum * (int64_t)sizeof(double) : 0) +
               (status ? nm * (int64_t)sizeof(int) : 0);
     CUDA_TRY(cudaStreamSynchronize(C->stream));
@@ -776,7 +790,7 @@ static void replan_batch(lcb_batch* B) {
     const bool same = !B->broken && P.shape_key == B->plan.shape_key;
     std::swap(B->plan, P);
     try {
-        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same);
+        upload_plan(C, B->dev, B->plan, B->data.data(), (int64_t)B->data.size(), !same, same ? &P : nullptr);
         if (!same && B->graph) {
             cudaGraphExecDestroy(B->graph);
             B->graph = nullptr;
@@ -870,8 +884,7 @@ int lcb_batch_run(lcb_batch* B, int scale) {
         }
         Range r("lcb batch run");
         CUDA_TRY(cudaGraphLaunch(B->graph, C->stream));
-        fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status);
-        CUDA_TRY(cudaMemcpy(B->ecount, B->dev.ecount.p, sizeof(B->ecount), cudaMemcpyDeviceToHost));
+        fetch_results(C, B->dev, B->plan, B->h_results, nullptr, &B->h_status, B->ecount);
         B->ran = true;
         for (int s : B->h_status)
             check_device_status(s);
