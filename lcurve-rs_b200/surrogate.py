@@ -83,7 +83,8 @@ class CurveEngine:
     """Resident batches of the setup's model for a few batch sizes; evaluates
     (N x 5) parameter rows to light curves or chi-squared against data."""
 
-    def __init__(self, setup: CurveSetup, data: np.ndarray | None = None, sizes=(8, 16, 32, 64, 128)):
+    def __init__(self, setup: CurveSetup, data: np.ndarray | None = None,
+                 sizes=(4, 8, 12, 16, 24, 32, 48, 64, 96, 128)):
         self.setup = setup
         base = Model(text=setup.text)
         if data is None:
