@@ -390,6 +390,13 @@ class Batch:
         check(_capi.load().lcb_batch_profile(self._h, int(bool(scale))))
         return self.stage_ms()
 
+    def chisq(self) -> np.ndarray:
+        """The last run's chi-squared per model (NaN for a failed model), without the
+        other result fields."""
+        out = np.empty(self.n)
+        check(_capi.load().lcb_batch_results(self._h, dptr(out), None, None))
+        return out
+
     def results(self, want_calc=False):
         chisq = np.zeros(self.n)
         calc = np.zeros(self._data.shape[0]) if want_calc else None

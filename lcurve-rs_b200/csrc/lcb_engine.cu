@@ -795,7 +795,9 @@ static void replan_batch(lcb_batch* B) {
             cudaGraphExecDestroy(B->graph);
             B->graph = nullptr;
         }
-        CUDA_TRY(cudaStreamSynchronize(C->stream));
+        // copies from pageable host memory are staged before cudaMemcpyAsync returns, so the
+        // plan's host tables may change at once; a new shape waits for its uploads here
+        if (!same) CUDA_TRY(cudaStreamSynchronize(C->stream));
     } catch (...) {
         cudaStreamSynchronize(C->stream);
         if (B->graph) cudaGraphExecDestroy(B->graph);

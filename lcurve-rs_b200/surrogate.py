@@ -116,8 +116,10 @@ class CurveEngine:
         b.set_params(PARAMS, pad)
         b.run(scale=scale)
         self.evals += n
-        chisq, calc, _ = b.results(want_calc=want_calc)
-        return chisq[:n], (calc.reshape(size, -1)[:n] if want_calc else None)
+        if not want_calc:
+            return b.chisq()[:n], None
+        chisq, calc, _ = b.results(want_calc=True)
+        return chisq[:n], calc.reshape(size, -1)[:n]
 
     def chisq(self, theta: np.ndarray, scale: bool = True) -> np.ndarray:
         return self._run(theta, scale, False)[0]
