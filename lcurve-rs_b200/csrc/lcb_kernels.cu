@@ -71,6 +71,9 @@ constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per l
 #define LCB_TUBE_MAX 8
 #endif
 constexpr int kTubeMax = LCB_TUBE_MAX;  // scan steps per phase-block miss proof (1: single steps only)
+#ifndef LCB_SPLIT_TUBES
+#define LCB_SPLIT_TUBES 0  // phase blocks in the split scan of small batches (slower there: 0)
+#endif
 #ifndef LCB_TUBE_BUDGET
 #define LCB_TUBE_BUDGET 24
 #endif
@@ -966,6 +969,35 @@ __device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double d
     const int total = sc.nsteps + 1, len = (total + split - 1) / split;
     const int lo = chunk * len, hi = min(total, lo + len);
     Los L{px, py, pz, 0.0, 0.0, 0.0};
+#if LCB_SPLIT_TUBES
+    int blk = kTubeMax, wait = 0, n = 0;  // phase blocks as in ingress_egress
+    for (int i = lo; i < hi; ++n) {
+        if ((n & 7) == 0 && *(volatile int*)first < lo) return;
+        const int last = wait > 0 ? i : min(i + blk - 1, hi - 1);
+        if (last > i) {
+            earth_at(cosi, sini, sc.phi1 + 0.5 * (double)(i + last) * sc.dphi, L.ex, L.ey, L.ez);
+            if (tube_miss(s, sc.acc, L, tube_width(sini, 0.5 * (double)(last - i) * sc.dphi), kTubeBudget, evals.cert)) {
+                ++evals.skipped;
+                i = last + 1;
+                blk = min(2 * blk, kTubeMax);
+            } else {
+                blk >>= 1;
+                if (blk < 2) wait = kTubeCool;
+            }
+            continue;
+        }
+        earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
+        const bool hit = fblink(s, sc.acc, L, evals, capped, kCertBudget);
+        if (capped) return;
+        if (hit) {
+            atomicMin(first, i);
+            return;
+        }
+        ++i;
+        if (wait > 0) --wait;
+        if (wait == 0) blk = max(blk, min(2, kTubeMax));
+    }
+#else
     for (int i = lo; i < hi; ++i) {
         if (((i - lo) & 7) == 0 && *(volatile int*)first < lo) return;
         earth_at(cosi, sini, sc.phi1 + (double)i * sc.dphi, L.ex, L.ey, L.ez);
@@ -976,6 +1008,7 @@ __device__ void scan_chunk(const RocheEcl& s, double cosi, double sini, double d
             return;
         }
     }
+#endif
 }
 
 __device__ __forceinline__ void roche_counters(const ElemArgs& A, const EclCount& cnt) {
