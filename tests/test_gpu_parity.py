@@ -152,6 +152,23 @@ def test_ragged_batch_and_resident_batch_vs_oracle(lcb, oracle, W):
         om.set("q", q[i])
         c = om.light_curve(data[offs[i]:offs[i + 1]], rdata=True, nthreads=8)["chisq"]
         assert abs(bchi3[i] - c) <= 1e-4 * abs(c)
+    # several re-parameterisations in a row (a re-plan uploads only the tables that changed):
+    # each equals a batch built fresh with those parameters
+    rng = np.random.default_rng(7)
+    names = ["q", "iangle", "r1", "t1", "t2"]
+    for _ in range(3):
+        vals = np.column_stack([rng.uniform(0.2, 0.9, len(models)), rng.uniform(78.0, 89.0, len(models)),
+                                rng.uniform(0.008, 0.025, len(models)), rng.uniform(9000.0, 30000.0, len(models)),
+                                rng.uniform(2600.0, 4800.0, len(models))])
+        B.set_params(names, vals)
+        B.run(scale=False)
+        fresh = [lcb.Model(text=s) for s, _ in specs]
+        for f, v in zip(fresh, vals):
+            for k, x in zip(names, v):
+                f.set_param(k, float(x))
+        F = lcb.Batch(fresh, data, offs)
+        F.run(scale=False)
+        assert np.allclose(B.chisq(), F.chisq(), rtol=1e-12, atol=0)
 
 
 @pytest.mark.parametrize("scale", [False, True])
