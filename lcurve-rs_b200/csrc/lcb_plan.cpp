@@ -763,7 +763,8 @@ class HostPool {
         int helpers = 0, users = 0;  // workers allowed / working on it (under the pool mutex)
     };
     std::mutex mu_;
-    std::condition_variable cv_;
+    std::condition_variable work_cv_;  // workers wait here for a job with items left
+    std::condition_variable done_cv_;  // callers of run() wait here for their job's end
     std::vector<Job*> open_;
 
     Job* pick() {
@@ -776,7 +777,7 @@ class HostPool {
             (*j->f)(i);
             if (j->done.fetch_add(1) + 1 == j->n) {
                 std::lock_guard<std::mutex> g(mu_);
-                cv_.notify_all();
+                done_cv_.notify_all();
             }
         }
     }
@@ -790,11 +791,11 @@ public:
                     Job* j = nullptr;
                     {
                         std::unique_lock<std::mutex> lk(mu_);
-                        cv_.wait(lk, [&] { return (j = pick()) != nullptr; });
+                        work_cv_.wait(lk, [&] { return (j = pick()) != nullptr; });
                     }
                     work(j);
                     std::lock_guard<std::mutex> g(mu_);
-                    if (--j->users == 0) cv_.notify_all();
+                    if (--j->users == 0) done_cv_.notify_all();
                 }
             }).detach();  // process-lifetime workers
     }
@@ -811,12 +812,13 @@ public:
             std::lock_guard<std::mutex> g(mu_);
             open_.push_back(&j);
         }
-        cv_.notify_all();
+        // wake only as many workers as can take an item (the caller works too)
+        for (int64_t k = 0; k < std::min<int64_t>(helpers, n - 1); ++k) work_cv_.notify_one();
         work(&j);
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return j.done.load() == n; });
+        done_cv_.wait(lk, [&] { return j.done.load() == n; });
         open_.erase(std::find(open_.begin(), open_.end(), &j));
-        cv_.wait(lk, [&] { return j.users == 0; });
+        done_cv_.wait(lk, [&] { return j.users == 0; });
     }
 };
 
@@ -875,14 +877,15 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
             }
         });
     }
-    // models are independent: prepare them on the host's cores (~40 us each)
-    parallel_for(n, 1, prep);
+    // models are independent: prepare them on the host's cores, 16 at least per thread
+    // (one takes ~10 us, so waking helper threads only pays off for larger batches)
+    parallel_for(n, 16, prep);
     // sub-phases and data: per-model sums, prefix offsets, then the per-datum
     // arrays of each model filled in parallel
     std::vector<int64_t> dbeg(n + 1, 0), sbeg(n + 1, 0);
     for (int64_t i = 0; i < n; ++i) dbeg[i + 1] = dbeg[i] + std::max<int64_t>(count[i], 0);
     P.ndatum = dbeg[n];
-    parallel_for(n, 16, [&](int64_t i) {
+    parallel_for(n, 64, [&](int64_t i) {
         int64_t ns = 0;
         if (P.model_ok[i])
             for (int64_t k = 0; k < dbeg[i + 1] - dbeg[i]; ++k) ns += std::max(data[start[i] + k].ndiv, 0);
@@ -895,7 +898,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     P.datum_model.resize(P.ndatum);
     P.datum_sub0.resize(P.ndatum);
     P.datum_src.resize(P.ndatum);
-    parallel_for(n, 16, [&](int64_t i) {
+    parallel_for(n, 64, [&](int64_t i) {
         ModelDev& D = lay[i].dev;
         D.datum_begin = dbeg[i];
         D.ndatum = dbeg[i + 1] - dbeg[i];
@@ -929,7 +932,7 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
     P.bands.resize(band_begin[n]);
     P.rings.resize(ring_begin[n]);
     P.nelem = elem_begin[n];
-    parallel_for(n, 8, [&](int64_t i) {
+    parallel_for(n, 64, [&](int64_t i) {
         const ModelLayout& L = lay[i];
         std::copy(L.bands.begin(), L.bands.end(), P.bands.begin() + band_begin[i]);
         std::copy(L.rings.begin(), L.rings.end(), P.rings.begin() + ring_begin[i]);
