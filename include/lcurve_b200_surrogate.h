@@ -110,6 +110,17 @@ int  lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y
                             const float* mean_dev, const float* sd_dev, const double* flux_dev,
                             const double* ferr_dev, int scale, int move, const double* kde_chol,
                             const double* kde_prec);
+/* The same sub-chain with y, ls, comp and rnd in host memory (no reference
+ * counterpart): the library stages them through one page-locked buffer of the
+ * network (one host-to-device copy in, one device-to-host copy of y and ls
+ * out, grown on first use outside any capture) and returns with y and ls
+ * updated.  Calls on one network must not overlap. */
+int  lcb_surrogate_subchain_host(lcb_mlp* net, int64_t n, int64_t m, int d, double* y, double* ls,
+                                 const double* comp, const double* rnd, int steps, double a, const double* lo,
+                                 const double* hi, const int* recip, const float* fmul, const float* fadd,
+                                 const float* mean_dev, const float* sd_dev, const double* flux_dev,
+                                 const double* ferr_dev, int scale, int move, const double* kde_chol,
+                                 const double* kde_prec);
 
 #ifdef __cplusplus
 }

@@ -54,8 +54,8 @@ SYMBOLS = [
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
     "lcb_mlp_train_step", "lcb_mlp_grads_device", "lcb_mlp_adam_step", "lcb_mlp_take_loss", "lcb_mlp_sync",
-    "lcb_mlp_gemm", "lcb_logflux_chisq", "lcb_surrogate_subchain", "lcb_mlp_state_size", "lcb_mlp_get_state",
-    "lcb_mlp_set_state",
+    "lcb_mlp_gemm", "lcb_logflux_chisq", "lcb_surrogate_subchain", "lcb_surrogate_subchain_host",
+    "lcb_mlp_state_size", "lcb_mlp_get_state", "lcb_mlp_set_state",
 ]
 
 _lib = None
@@ -129,6 +129,8 @@ def load():
         "lcb_logflux_chisq": ([i64, i, vp, vp, vp, vp, vp, i, vp, vp], i),
         "lcb_surrogate_subchain": ([vp, i64, i64, i, vp, vp, vp, vp, i, d, dp, dp, C.POINTER(i),
                                     C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, vp, vp, i, i, dp, dp], i),
+        "lcb_surrogate_subchain_host": ([vp, i64, i64, i, vp, vp, vp, vp, i, d, dp, dp, C.POINTER(i),
+                                         C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, vp, vp, i, i, dp, dp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -859,6 +859,9 @@ struct lcb_mlp {
     DBuf<double> sub_lq, sub_lqp;          // KDE log densities (current, proposed)
     DBuf<double> sub_kde;                  // KDE factors of the current call
     DBuf<double> sub_y, sub_ls, sub_comp, sub_rnd;  // fixed copies of the sub-chain's inputs (graph operands)
+    DBuf<double> sub_stage;                // lcb_surrogate_subchain_host: device side of the staging
+    double* sub_pinned = nullptr;          // ... and its page-locked host side
+    size_t sub_pinned_n = 0;
     cudaGraphExec_t sub_graph = nullptr;   // the captured K-step sub-chain
     std::vector<unsigned char> sub_key;    // what the captured graph depends on
     int64_t steps = 0;
@@ -875,7 +878,10 @@ struct lcb_mlp {
         wsplit.free();
         dz[0].free(); dz[1].free(); err.free(); loss.free();
         sub_x.free(); sub_yp.free(); sub_lz.free(); sub_chi.free(); sub_lq.free(); sub_lqp.free(); sub_kde.free();
-        sub_y.free(); sub_ls.free(); sub_comp.free(); sub_rnd.free();
+        sub_y.free(); sub_ls.free(); sub_comp.free(); sub_rnd.free(); sub_stage.free();
+        if (sub_pinned) cudaFreeHost(sub_pinned);
+        sub_pinned = nullptr;
+        sub_pinned_n = 0;
         if (sub_graph) cudaGraphExecDestroy(sub_graph);
         sub_graph = nullptr;
         for (auto& t : y) t.free();
@@ -1347,6 +1353,54 @@ int lcb_surrogate_subchain(lcb_mlp* net, int64_t n, int64_t m, int d, double* y_
         CK(cudaGraphLaunch(net->sub_graph, st));
         CK(cudaMemcpyAsync(y_dev, net->sub_y.p, n * d * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ls_dev, net->sub_ls.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    });
+}
+
+int lcb_surrogate_subchain_host(lcb_mlp* net, int64_t n, int64_t m, int d, double* y, double* ls, const double* comp,
+                                const double* rnd, int steps, double a, const double* lo, const double* hi,
+                                const int* recip, const float* fmul, const float* fadd, const float* mean_dev,
+                                const float* sd_dev, const double* flux_dev, const double* ferr_dev, int scale, int move,
+                                const double* kde_chol, const double* kde_prec) {
+    if (!net || !y || !ls || !comp || !rnd) return LCB_ERR_INVALID;
+    if (n <= 0 || m <= 0 || d <= 0 || steps < 0 || n > net->max_batch || m > net->max_batch || d > kMaxDim)
+        return LCB_ERR_INVALID;
+    const int rstride = move == MOVE_KDE ? 3 + d : 3;
+    const size_t ny = (size_t)n * d, nc = (size_t)m * d, nr = (size_t)steps * n * rstride;
+    const size_t total = ny + n + nc + nr;  // [y | ls | comp | rnd], doubles
+    int rc = guard([&] {
+        CK(cudaSetDevice(net->device));
+        if (net->sub_pinned_n < total) {  // grow both sides of the staging (outside any capture)
+            const size_t want = std::max<size_t>(total, 2 * net->sub_pinned_n);
+            CK(cudaStreamSynchronize(net->stream));
+            if (net->sub_pinned) CK(cudaFreeHost(net->sub_pinned));
+            net->sub_pinned = nullptr;
+            net->sub_pinned_n = 0;
+            net->sub_stage.free();
+            CK(cudaMallocHost((void**)&net->sub_pinned, want * sizeof(double)));
+            net->sub_pinned_n = want;
+            net->sub_stage.alloc(want);
+        }
+        double* h = net->sub_pinned;
+        std::memcpy(h, y, ny * sizeof(double));
+        std::memcpy(h + ny, ls, n * sizeof(double));
+        std::memcpy(h + ny + n, comp, nc * sizeof(double));
+        std::memcpy(h + ny + n + nc, rnd, nr * sizeof(double));
+        CK(cudaMemcpyAsync(net->sub_stage.p, h, total * sizeof(double), cudaMemcpyHostToDevice, net->stream));
+    });
+    if (rc != LCB_OK) return rc;
+    double* dv = net->sub_stage.p;
+    rc = lcb_surrogate_subchain(net, n, m, d, dv, dv + ny, dv + ny + n, dv + ny + n + nc, steps, a, lo, hi, recip,
+                                fmul, fadd, mean_dev, sd_dev, flux_dev, ferr_dev, scale, move, kde_chol, kde_prec);
+    if (rc != LCB_OK) {
+        cudaStreamSynchronize(net->stream);  // the staging is reused by the next call
+        return rc;
+    }
+    return guard([&] {
+        double* h = net->sub_pinned;
+        CK(cudaMemcpyAsync(h, dv, (ny + n) * sizeof(double), cudaMemcpyDeviceToHost, net->stream));
+        CK(cudaStreamSynchronize(net->stream));
+        std::memcpy(y, h, ny * sizeof(double));
+        std::memcpy(ls, h + ny, n * sizeof(double));
     });
 }
 

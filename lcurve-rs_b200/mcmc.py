@@ -86,10 +86,12 @@ class KDE:
         """bandwidth multiplies Scott's factor (1 = emcee's default)."""
         m, d = comp.shape
         h2 = (bandwidth * m ** (-1.0 / (d + 4))) ** 2
-        cov = np.cov(comp, rowvar=False) * h2
-        cov = cov + np.diag(1e-12 * np.diag(cov) + 1e-300)
+        c = comp - comp.mean(axis=0)
+        cov = (c.T @ c) * (h2 / (m - 1))  # the sample covariance (np.cov's), scaled
+        cov[np.diag_indices(d)] += 1e-12 * np.diag(cov) + 1e-300
         chol = np.linalg.cholesky(cov)
-        return cls(comp, chol, np.linalg.inv(cov), np.linalg.inv(chol))
+        white = np.linalg.inv(chol)
+        return cls(comp, chol, white.T @ white, white)
 
     def logq(self, y: np.ndarray) -> np.ndarray:
         # squared Mahalanobis distances |a - b|^2 = |a|^2 + |b|^2 - 2 a.b of whitened points, centred

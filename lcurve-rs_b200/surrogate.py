@@ -383,8 +383,7 @@ class Surrogate:
                  scale: bool = True, move: str = "stretch", bandwidth: float = 1.0):
         """Runs rnd.shape[0] surrogate Metropolis moves (stretch or KDE) of the
         walkers y (log probabilities ls) against the fixed walkers comp on the
-        device (lcb_surrogate_subchain); returns the new (y, ls)."""
-        torch = _torch()
+        device (lcb_surrogate_subchain_host); returns the new (y, ls)."""
         from .mcmc import KDE  # noqa: PLC0415
         y = np.ascontiguousarray(y, dtype=np.float64)
         n, d = y.shape
@@ -398,40 +397,17 @@ class Surrogate:
             keep = ()
         comp = np.ascontiguousarray(comp, dtype=np.float64)
         m = comp.shape[0]
-        # one pinned staging buffer, one copy each way: [y (n x d), ls (n), comp (m x d), rnd]
-        sizes = (n * d, n, m * d, rnd.size)
-        offs = np.cumsum((0,) + sizes)
-        buf_h, buf_d = self._staging(int(offs[-1]))
-        h = buf_h.numpy()
-        h[offs[0]:offs[1]] = y.ravel()
-        h[offs[1]:offs[2]] = ls
-        h[offs[2]:offs[3]] = comp.ravel()
-        h[offs[3]:offs[4]] = np.asarray(rnd, dtype=np.float64).ravel()
-        base = buf_d.data_ptr()
-        ptr = [C.c_void_p(base + 8 * int(o)) for o in offs[:4]]
-        with torch.cuda.stream(self._stream):
-            buf_d[:offs[4]].copy_(buf_h[:offs[4]], non_blocking=True)
-            _capi.check_mlp(self.L.lcb_surrogate_subchain(
-                self._h, n, m, d, ptr[0], ptr[1], ptr[2], ptr[3], rnd.shape[0], a, self._c_lo, self._c_hi,
-                self._c_recip, self._c_fmul, self._c_fadd, C.c_void_p(self.mean.data_ptr()),
-                C.c_void_p(self.sd.data_ptr()), C.c_void_p(self._flux.data_ptr()), C.c_void_p(self._ferr.data_ptr()),
-                int(bool(scale)), 1 if move == "kde" else 0, chol, prec))
-            out = self._out_h[:offs[2]]
-            out.copy_(buf_d[:offs[2]], non_blocking=True)
-        self._stream.synchronize()
+        y = y.copy()
+        ls = np.array(ls, dtype=np.float64)
+        rnd = np.ascontiguousarray(rnd, dtype=np.float64)
+        # host arrays in and out: the library stages them through its own page-locked buffer
+        _capi.check_mlp(self.L.lcb_surrogate_subchain_host(
+            self._h, n, m, d, y.ctypes.data, ls.ctypes.data, comp.ctypes.data, rnd.ctypes.data, rnd.shape[0], a,
+            self._c_lo, self._c_hi, self._c_recip, self._c_fmul, self._c_fadd, C.c_void_p(self.mean.data_ptr()),
+            C.c_void_p(self.sd.data_ptr()), C.c_void_p(self._flux.data_ptr()), C.c_void_p(self._ferr.data_ptr()),
+            int(bool(scale)), 1 if move == "kde" else 0, chol, prec))
         del keep
-        o = out.numpy()
-        return o[:n * d].reshape(n, d).copy(), o[n * d:n * d + n].copy()
-
-    def _staging(self, count: int):
-        """Pinned host and device buffers of at least `count` doubles (kept across calls)."""
-        torch = _torch()
-        if getattr(self, "_stage_n", 0) < count:
-            self._stage_n = max(count, 2 * getattr(self, "_stage_n", 0))
-            self._stage_h = torch.empty(self._stage_n, dtype=torch.float64, pin_memory=True)
-            self._stage_d = torch.empty(self._stage_n, dtype=torch.float64, device=self.dev)
-            self._out_h = torch.empty(self._stage_n, dtype=torch.float64, pin_memory=True)
-        return self._stage_h, self._stage_d
+        return y, ls
 
 
 def refine_near(sur: Surrogate, setup: CurveSetup, ensemble: np.ndarray, theta_global: np.ndarray,
