@@ -66,6 +66,14 @@ constexpr double kEfac = 1.0000001;                               // grid.rs:396
 #define LCB_CERT_BUDGET 32
 #endif
 constexpr int kRocheMinBlocks = LCB_ROCHE_MIN_BLOCKS;  // k_roche blocks per SM (128 threads): register budget
+#ifndef LCB_SCAN_MIN_BLOCKS
+#define LCB_SCAN_MIN_BLOCKS LCB_ROCHE_MIN_BLOCKS
+#endif
+#ifndef LCB_CHOP_MIN_BLOCKS
+#define LCB_CHOP_MIN_BLOCKS LCB_ROCHE_MIN_BLOCKS
+#endif
+constexpr int kScanMinBlocks = LCB_SCAN_MIN_BLOCKS;  // the same for the split scan (small batches)
+constexpr int kChopMinBlocks = LCB_CHOP_MIN_BLOCKS;  // and for its bisection kernel
 constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per line of sight before the full search
 #ifndef LCB_TUBE_MAX
 #define LCB_TUBE_MAX 8
@@ -1025,7 +1033,7 @@ __device__ __forceinline__ void roche_counters(const ElemArgs& A, const EclCount
 // Split scan, first kernel: block b scans chunk b % split of the elements of
 // Roche block b / split.  For small batches, whose time is otherwise the
 // longest single scan, this spreads each scan over `split` threads.
-__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(ElemArgs A) {
+__global__ void __launch_bounds__(kRocheBlock, kScanMinBlocks) k_roche_scan(ElemArgs A) {
     const int64_t rb = blockIdx.x / A.roche_split;
     const int chunk = (int)(blockIdx.x % A.roche_split);
     const ElemBlock blk = A.rblocks[rb];
@@ -1050,7 +1058,7 @@ __global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_scan(Ele
 // first hit, eclipse.rs:301-332), halving the longest chain of line-of-sight
 // searches; the ingress lane combines the pair.  Block b covers half of Roche
 // block b / 2.
-__global__ void __launch_bounds__(kRocheBlock, kRocheMinBlocks) k_roche_chop2(ElemArgs A) {
+__global__ void __launch_bounds__(kRocheBlock, kChopMinBlocks) k_roche_chop2(ElemArgs A) {
     const int64_t rb = blockIdx.x >> 1;
     const int slot = (int)(blockIdx.x & 1) * (kRocheBlock / 2) + (int)(threadIdx.x >> 1);
     const int part = threadIdx.x & 1;  // 0: ingress, 1: egress
