@@ -240,6 +240,14 @@ int  lcb_batch_stage_ms(const lcb_batch* b, double* out6);
  * (the reference's chisq_batch model loop, orchestration.rs:343-356) weigh
  * models with it. */
 int lcb_model_work(const lcb_model* model, const lcb_datum* data, int64_t n, int64_t* out4);
+/* Bright-spot positions: the gas stream from L1 integrated to each radius[i] for
+ * mass ratio q[i] (replaces crates/roche/src/stream.rs:82-145 stradv as
+ * crates/lcurve/src/grid.rs:494 calls it), out[3 i ..] = (x, y, z), on the host
+ * (on_device = 0) or one GPU thread per pair on the context's device (1), the
+ * same source compiled for both.  Planning uses the GPU path itself for a batch
+ * with more new (q, radius) pairs than four per host thread.  Rows whose stream
+ * fails are NaN and the call returns LCB_ERR_MODEL. */
+int lcb_stream_points(lcb_ctx* ctx, const double* q, const double* radius, int64_t n, int on_device, double* out);
 
 /* ---- failure-path hooks (no reference counterpart) ------------------------
  * The eclipse search bounds one line-of-sight search at 262,144 potential

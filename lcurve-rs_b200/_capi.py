@@ -49,7 +49,7 @@ SYMBOLS = [
     "lcb_batch_set_params", "lcb_batch_run", "lcb_batch_results", "lcb_batch_stats", "lcb_batch_profile", "lcb_batch_stage_ms",
     "lcb_ctx_transfer_bytes", "lcb_measure_fma_peak", "lcb_model_grid", "lcb_batch_search_counts",
     "lcb_light_curve_noalloc", "lcb_batch_set_tuning", "lcb_batch_get_tuning", "lcb_ctx_set_search_cap",
-    "lcb_wait_probe", "lcb_model_work", "lcb_model_elements", "lcb_light_curve_elements",
+    "lcb_wait_probe", "lcb_model_work", "lcb_model_elements", "lcb_light_curve_elements", "lcb_stream_points",
     # surrogate (lcurve_b200_surrogate.h)
     "lcb_mlp_last_error", "lcb_mlp_create", "lcb_mlp_destroy", "lcb_mlp_set_stream", "lcb_mlp_num_params",
     "lcb_mlp_get_params", "lcb_mlp_set_params", "lcb_mlp_get_grads", "lcb_mlp_forward", "lcb_mlp_backward",
@@ -105,6 +105,7 @@ def load():
         "lcb_ctx_set_search_cap": ([vp, i], i),
         "lcb_wait_probe": ([vp, i64, i64p], i),
         "lcb_model_work": ([vp, vp, i64, i64p], i),
+        "lcb_stream_points": ([vp, dp, dp, i64, i, dp], i),
         "lcb_model_elements": ([vp, vp, i64, i64, vp, vp, vp, vp, vp, i64p], i),
         "lcb_light_curve_elements": ([vp, vp, vp, i64, i, i, vp, vp, vp, vp, vp, dp, C.POINTER(Result)], i),
         "lcb_mlp_last_error": ([], cp),

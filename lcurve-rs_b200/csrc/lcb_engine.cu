@@ -22,6 +22,7 @@
 #include "lcb_kernels.cuh"
 #include "lcb_model.h"
 #include "lcb_plan.h"
+#include "lcb_stream.h"
 
 using lcb::Error;
 
@@ -960,6 +961,59 @@ int lcb_ctx_transfer_bytes(const lcb_ctx* C, int64_t* h2d, int64_t* d2h) {
     *h2d = C->h2d;
     *d2h = C->d2h;
     return LCB_OK;
+}
+
+namespace {
+
+// The planner's GPU path for many bright-spot streams (lcb_plan.h: StreamDeviceFn): one
+// k_stream launch on the calling thread's default stream of the current device; false on
+// any CUDA error (the planner then integrates on the host).
+bool stream_on_device(const double* in, int n, double* out, int* status) {
+    if (n <= 0) return true;
+    char* buf = nullptr;
+    const size_t bin = 3 * sizeof(double) * (size_t)n, bst = sizeof(int) * (size_t)n;
+    cudaStream_t s = cudaStreamPerThread;
+    bool ok = cudaMalloc(&buf, 2 * bin + bst) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(buf, in, bin, cudaMemcpyHostToDevice, s) == cudaSuccess;
+    ok = ok && lcb::launch_stream((const double*)buf, n, (double*)(buf + bin), (int*)(buf + 2 * bin), s) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(out, buf + bin, bin, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(status, buf + 2 * bin, bst, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (buf) cudaFree(buf);
+    if (!ok) cudaGetLastError();  // clear a non-sticky error; the host path takes over
+    return ok;
+}
+
+const bool g_stream_device_registered = (lcb::set_stream_device(&stream_on_device), true);
+
+}  // namespace
+
+int lcb_stream_points(lcb_ctx* C, const double* q, const double* radius, int64_t n, int on_device, double* out) {
+    if (!C || (n > 0 && (!q || !radius || !out)) || n < 0 || n > (1 << 24)) return fail(LCB_ERR_INVALID, "bad arguments");
+    return guarded(C, [&] {
+        (void)g_stream_device_registered;
+        std::vector<double> in(3 * n);
+        std::vector<int> st(n, lcb::stream::kStreamOk);
+        for (int64_t i = 0; i < n; ++i) {
+            in[3 * i] = q[i];
+            in[3 * i + 1] = lcb::host_xl1(q[i]);
+            in[3 * i + 2] = radius[i];
+        }
+        if (on_device) {
+            if (!stream_on_device(in.data(), (int)n, out, st.data()))
+                throw Error(LCB_ERR_CUDA, "the gas-stream kernel failed");
+        } else {
+            for (int64_t i = 0; i < n; ++i)
+                st[i] = lcb::stream::stream_to_radius_core(q[i], in[3 * i + 1], radius[i], out + 3 * i);
+        }
+        bool bad = false;
+        for (int64_t i = 0; i < n; ++i)
+            if (st[i] != lcb::stream::kStreamOk) {
+                out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = NAN;
+                bad = true;
+            }
+        if (bad) throw Error(LCB_ERR_MODEL, "the gas stream did not reach a radius (NaN rows)");
+    });
 }
 
 int lcb_model_work(const lcb_model* model, const lcb_datum* data, int64_t n, int64_t* out4) {

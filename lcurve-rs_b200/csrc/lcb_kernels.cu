@@ -39,6 +39,7 @@
 #include <cstdint>
 
 #include "lcb_kernels.cuh"
+#include "lcb_stream.h"
 
 namespace lcb {
 
@@ -2085,6 +2086,24 @@ cudaError_t launch_ecl_export(const double2* ecl, int64_t nelem, int64_t first, 
 cudaError_t launch_ecl_import(const double2* in, int64_t nelem, double2* ecl, unsigned* ecl_grp, cudaStream_t s) {
     const int64_t n = nelem * kMaxEcl;
     if (n > 0) k_ecl_import<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, nelem, ecl, ecl_grp);
+    return cudaGetLastError();
+}
+
+// The bright spot's gas-stream end point for pair i (lcb_stream.h, the planner's
+// host code compiled for the device): one thread per pair, each in a block of its
+// own, since every integration is one long serial chain of FP64 operations and
+// the pairs' step sequences differ (lanes of one warp would diverge).
+__global__ void __launch_bounds__(1) k_stream(const double* __restrict__ in, int n, double* __restrict__ out,
+                                              int* __restrict__ status) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    double o[3] = {0.0, 0.0, 0.0};
+    status[i] = stream::stream_to_radius_core(in[3 * i], in[3 * i + 1], in[3 * i + 2], o);
+    out[3 * i] = o[0]; out[3 * i + 1] = o[1]; out[3 * i + 2] = o[2];
+}
+
+cudaError_t launch_stream(const double* in, int n, double* out, int* status, cudaStream_t s) {
+    if (n > 0) k_stream<<<(unsigned)n, 1, 0, s>>>(in, n, out, status);
     return cudaGetLastError();
 }
 

@@ -104,6 +104,8 @@ cudaError_t measure_fma_peak(int fp64, int num_sms, cudaStream_t s, double* tflo
 cudaError_t launch_ecl_export(const double2* ecl, int64_t nelem, int64_t first, int64_t count, double2* out,
                               cudaStream_t s);
 cudaError_t launch_ecl_import(const double2* in, int64_t nelem, double2* ecl, unsigned* ecl_grp, cudaStream_t s);
+// Gas-stream end points of n (q, L1 distance, radius) triples, one thread each (k_stream).
+cudaError_t launch_stream(const double* in, int n, double* out, int* status, cudaStream_t s);
 // One block waiting on an mbarrier that nothing completes, bounded by `limit` cycles.
 cudaError_t launch_wait_probe(long long limit, int* status, long long* waited, cudaStream_t s);
 

@@ -10,6 +10,7 @@
 // element kernel and splits the flux sum into (element range x sub-phase
 // tile) work units for the persistent flux kernel.
 #include "lcb_plan.h"
+#include "lcb_stream.h"
 
 #include <algorithm>
 #include <array>
@@ -132,180 +133,11 @@ double dlpdlt(double wave, double temp) {
     return e / (1.0 - std::exp(-e));
 }
 
-// ---- gas stream: Bulirsch-Stoer with the reference's step control ---------
-class BulirschStoer {  // bsstep.rs:13-324
-public:
-    static constexpr int kK = 8;
-    template <class F>  // F(y, dydx): the right-hand side, inlined
-    void step(double* y, const double* dydx, double& x, double htry, double eps, double& hdid, double& hnext,
-              const F& f) {
-        static const int nseq[kK + 1] = {2, 4, 6, 8, 10, 12, 14, 16, 18};
-        const double safe1 = 0.25, safe2 = 0.7, redmax = 1.0e-5, redmin = 0.7, tiny = 1.0e-30, scalmx = 0.1;
-        double err[kK] = {0}, ysav[6], yseq[6], yerr[6];
-        double tab[6][kK + 1] = {{0}}, xt[kK + 1] = {0};
-        if (eps != epsold_) {
-            xnew_ = -1.0e29;
-            double eps1 = safe1 * eps;
-            a_[0] = nseq[0] + 1.0;
-            for (int k = 0; k < kK; ++k) a_[k + 1] = a_[k] + nseq[k + 1];
-            for (int iq = 1; iq < kK; ++iq)
-                for (int k = 0; k < iq; ++k)
-                    alf_[k][iq] = std::pow(eps1, (a_[k + 1] - a_[iq + 1]) / ((a_[iq + 1] - a_[0] + 1.0) * (2 * k + 3)));
-            epsold_ = eps;
-            kopt_ = 1;
-            for (int k = 1; k < kK - 1; ++k) {
-                kopt_ = k;
-                if (a_[k + 1] > a_[k] * alf_[k - 1][k]) break;
-            }
-            kmax_ = kopt_;
-        }
-        double h = htry;
-        for (int i = 0; i < 6; ++i) ysav[i] = y[i];
-        if (x != xnew_ || h != xnew_) { first_ = true; kopt_ = kmax_; }
-        bool reduct = false;
-        int km = 0;
-        for (;;) {
-            bool done = false;
-            for (int k = 0; k <= kmax_; ++k) {
-                xnew_ = x + h;
-                if (xnew_ == x) { hdid = 0.0; hnext = 0.0; return; }
-                midpoint(ysav, dydx, h, nseq[k], yseq, f);
-                double xest = sq(h / nseq[k]);
-                extrapolate(k, xest, yseq, y, yerr, tab, xt);
-                double errmax = 0.0;
-                if (k != 0) {
-                    errmax = tiny;
-                    for (int i = 0; i < 6; ++i) errmax = std::fmax(errmax, std::fabs(yerr[i]));
-                    errmax /= eps;
-                    km = k - 1;
-                    err[km] = std::pow(errmax / safe1, 1.0 / (2 * km + 3));
-                }
-                if (k != 0 && (k >= std::max(kopt_ - 1, 0) || first_)) {
-                    if (err[km] != 0.0 && errmax < 1.0) { done = true; break; }
-                    if (k == kmax_ || k == kopt_ + 1) break;
-                    if (k == kopt_ && alf_[kopt_ - 1][kopt_] < err[km]) break;
-                    if (kopt_ == kmax_ && alf_[km][kmax_ - 1] < err[km]) break;
-                    if (alf_[km][kopt_] < err[km]) break;
-                }
-            }
-            if (done) break;
-            double red = err[km] > 0.0 ? std::fmin(std::fmax(safe2 / err[km], redmax), redmin) : redmin;
-            h *= red;
-            reduct = true;
-        }
-        x = xnew_;
-        hdid = h;
-        first_ = false;
-        double wrkmin = 1.0e35, fac = 1.0;
-        for (int kk = 0; kk <= km; ++kk) {
-            double f2 = std::fmax(err[kk], scalmx), work = f2 * a_[kk + 1];
-            if (work < wrkmin) { fac = f2; wrkmin = work; kopt_ = kk + 1; }
-        }
-        hnext = h / fac;
-        if (kopt_ >= km + 1 && kopt_ != kmax_ && !reduct) {
-            double f2 = std::fmax(fac / alf_[kopt_ - 1][kopt_], scalmx);
-            if (a_[kopt_ + 1] * f2 <= wrkmin) { hnext = h / f2; kopt_ += 1; }
-        }
-    }
-
-private:
-    template <class F>
-    static void midpoint(const double* y, const double* dydx, double htot, int n, double* yout,
-                         const F& f) {  // bsstep.rs:57-93
-        double h = htot / n, ym[6], yn[6];
-        for (int i = 0; i < 6; ++i) { ym[i] = y[i]; yn[i] = y[i] + h * dydx[i]; }
-        f(yn, yout);
-        for (int s = 1; s < n; ++s) {
-            for (int i = 0; i < 6; ++i) { double t = ym[i] + 2.0 * h * yout[i]; ym[i] = yn[i]; yn[i] = t; }
-            f(yn, yout);
-        }
-        for (int i = 0; i < 6; ++i) yout[i] = 0.5 * (ym[i] + yn[i] + h * yout[i]);
-    }
-    static void extrapolate(int iest, double xest, const double* yest, double* yz, double* dy,
-                            double tab[6][kK + 1], double* xt) {  // bsstep.rs:96-149
-        xt[iest] = xest;
-        for (int j = 0; j < 6; ++j) { dy[j] = yest[j]; yz[j] = yest[j]; }
-        if (iest == 0) {
-            for (int j = 0; j < 6; ++j) tab[j][0] = yest[j];
-            return;
-        }
-        double c[6];
-        for (int j = 0; j < 6; ++j) c[j] = yest[j];
-        for (int k1 = 0; k1 < iest; ++k1) {
-            double d = 1.0 / (xt[iest - k1 - 1] - xest);
-            double f1 = xest * d, f2 = xt[iest - k1 - 1] * d;
-            for (int j = 0; j < 6; ++j) {
-                double qv = tab[j][k1];
-                tab[j][k1] = dy[j];
-                double dl = c[j] - qv;
-                dy[j] = f1 * dl;
-                c[j] = f2 * dl;
-                yz[j] += dy[j];
-            }
-        }
-        for (int j = 0; j < 6; ++j) tab[j][iest] = dy[j];
-    }
-    bool first_ = true;
-    int kmax_ = 0, kopt_ = 0;
-    double epsold_ = -1.0, xnew_ = -1.0e29, a_[kK + 1] = {0}, alf_[kK][kK] = {{0}};
-};
-
-// Acceleration in the rotating frame (misc.rs:4-19) as an ODE right-hand side.
-void roche_rhs(double q, const double* y, double* d) {
-    double f1 = 1.0 / (1.0 + q), f2 = f1 * q;
-    double yz = sq(y[1]) + sq(y[2]);
-    double r1sq = sq(y[0]) + yz, r2sq = sq(y[0] - 1.0) + yz;
-    double fm1 = f1 / (r1sq * std::sqrt(r1sq)), fm2 = f2 / (r2sq * std::sqrt(r2sq)), fm3 = fm1 + fm2;
-    d[0] = y[3]; d[1] = y[4]; d[2] = y[5];
-    d[3] = -fm3 * y[0] + fm2 + 2.0 * y[4] + y[0] - f2;
-    d[4] = -fm3 * y[1] - 2.0 * y[3] + y[1];
-    d[5] = -fm3 * y[2];
-}
-
-// One gsint step (stream.rs:26-62).
-void stream_step(double q, double* y, double& t, double htry, BulirschStoer& bs, double& hdid, double& hnext) {
-    double d[6];
-    roche_rhs(q, y, d);
-    bs.step(y, d, t, htry, 1.0e-8, hdid, hnext, [q](const double* yy, double* dd) { roche_rhs(q, yy, dd); });
-}
-
-inline double radius3(const double* y) { return std::sqrt(sq(y[0]) + sq(y[1]) + sq(y[2])); }
-
-// strinit + stradv(q, r, v, rad, 1e-10, 1e-3) (stream.rs:8-20, 82-145).
+// ---- gas stream (lcb_stream.h: the same source runs on the device) ----------
 void stream_to_radius_uncached(double q, double rad, double out[3]) {
-    const double small = 1.0e-5;
-    double rl1 = host_xl1(q), mu = q / (1.0 + q);
-    double a = (1.0 - mu) / cube(rl1) + mu / cube(1.0 - rl1);
-    double lam = std::sqrt(((a - 2.0) + std::sqrt(a * (9.0 * a - 8.0))) / 2.0);
-    double m1 = (lam * lam - 2.0 * a - 1.0) / (2.0 * lam);
-    double y[6] = {rl1 - small, -m1 * small, 0.0, -lam * small, -lam * m1 * small, 0.0};
-    BulirschStoer bs;
-    double rinit = radius3(y), t = 0.0, tnext = 1.0e-2;
-    for (;;) {
-        double yo[6];
-        std::memcpy(yo, y, sizeof yo);
-        double hdid, hn;
-        stream_step(q, y, t, std::fmin(tnext, 1.0e-3), bs, hdid, hn);
-        tnext = hn;
-        double rnow = radius3(y);
-        if ((rinit > rad && rnow <= rad) || (rinit < rad && rnow >= rad)) {
-            double lo = 0.0, hi = hdid, rlo = radius3(yo), rhi = rnow, t0 = t - hdid;
-            for (int guard = 0; std::fabs(rhi - rlo) > 1e-10; ++guard) {
-                if (guard > 100000) throw model_err("stradv: binary chop failed to converge");
-                double tm = (lo + hi) / 2.0;
-                std::memcpy(y, yo, sizeof yo);
-                double tt = t0, a1, a2;
-                BulirschStoer bs2;
-                stream_step(q, y, tt, tm, bs2, a1, a2);
-                rnow = radius3(y);
-                if ((rhi > rad && rnow > rad) || (rhi < rad && rnow < rad)) { rhi = rnow; hi = tm; }
-                else { rlo = rnow; lo = tm; }
-            }
-            out[0] = y[0]; out[1] = y[1]; out[2] = y[2];
-            return;
-        }
-        if (t > 10.0) throw model_err("stradv: took too long without crossing radius=" + std::to_string(rad));
-    }
+    const int rc = stream::stream_to_radius_core(q, host_xl1(q), rad, out);
+    if (rc == stream::kStreamChopFailed) throw model_err("stradv: binary chop failed to converge");
+    if (rc != stream::kStreamOk) throw model_err("stradv: took too long without crossing radius=" + std::to_string(rad));
 }
 
 // stream_to_radius_uncached memoised on (q, rad), process-wide: the integration is ~20,000
@@ -341,9 +173,7 @@ static bool spot_cached(double q, double rad, double out[3]) {
     return true;
 }
 
-void stream_to_radius(double q, double rad, double out[3]) {
-    if (spot_cached(q, rad, out)) return;
-    stream_to_radius_uncached(q, rad, out);
+static void spot_store(double q, double rad, const double out[3]) {
     std::lock_guard<std::mutex> g(g_spot_mu);
     const SpotKey k = spot_key(q, rad);
     if (g_spot_memo.emplace(k, std::array<double, 3>{out[0], out[1], out[2]}).second) {
@@ -353,6 +183,14 @@ void stream_to_radius(double q, double rad, double out[3]) {
             g_spot_order.pop_front();
         }
     }
+}
+
+static std::atomic<StreamDeviceFn> g_stream_device{nullptr};
+
+void stream_to_radius(double q, double rad, double out[3]) {
+    if (spot_cached(q, rad, out)) return;
+    stream_to_radius_uncached(q, rad, out);
+    spot_store(q, rad, out);
 }
 
 // Latitude bands of one star grid (grid.rs:157-322) appended to `bands`;
@@ -744,6 +582,9 @@ double host_xl12(double q, double spin) {
     return l1_newton(q, -s + mu, 3.0 * s + 2.0 * mu - 2.0, 1.0 - mu - 3.0 * s, s, "xl12");
 }
 void host_stream_spot(double q, double radius, double out[3]) { stream_to_radius(q, radius, out); }
+void set_stream_device(StreamDeviceFn fn) { g_stream_device.store(fn); }
+bool spot_memo_get(double q, double radius, double out[3]) { return spot_cached(q, radius, out); }
+void spot_memo_put(double q, double radius, const double out[3]) { spot_store(q, radius, out); }
 int64_t host_numface(int nlat) {
     std::vector<Band> b;
     Model m;
@@ -869,6 +710,31 @@ void plan_batch(const Model* const* models, int64_t n, const lcb_datum* data, co
         }
         std::sort(need.begin(), need.end());
         need.erase(std::unique(need.begin(), need.end()), need.end());
+        // many new pairs: one GPU thread each (a host core integrates one in ~0.7 ms, a GPU
+        // thread in a few; the GPU wins once the host would run more than four per thread)
+        const StreamDeviceFn dev = g_stream_device.load();
+        const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+        if (dev && (int64_t)need.size() > 4 * hw) {
+            std::vector<double> in, res(3 * need.size());
+            std::vector<int> st(need.size(), -1);
+            std::vector<size_t> which;
+            for (size_t k = 0; k < need.size(); ++k) {
+                try {
+                    const double rl1 = host_xl1(need[k].first);
+                    in.insert(in.end(), {need[k].first, rl1, need[k].second});
+                    which.push_back(k);
+                } catch (const std::exception&) {  // the model's own planning reports it
+                }
+            }
+            if (!which.empty() && dev(in.data(), (int)which.size(), res.data(), st.data())) {
+                std::vector<std::pair<double, double>> rest;
+                for (size_t j = 0; j < which.size(); ++j) {
+                    if (st[j] == stream::kStreamOk) spot_store(need[which[j]].first, need[which[j]].second, &res[3 * j]);
+                    else rest.push_back(need[which[j]]);  // failures: the host path reports them
+                }
+                need.swap(rest);
+            }
+        }
         parallel_for((int64_t)need.size(), 1, [&](int64_t k) {
             double o[3];
             try {

@@ -68,6 +68,17 @@ double host_xl1(double q);
 double host_xl11(double q, double spin);
 double host_xl12(double q, double spin);
 void host_stream_spot(double q, double radius, double out[3]);
+
+// Gas-stream end points on a GPU for many (q, radius) pairs at once: in[3 i ..] = (q,
+// L1 distance, radius), out[3 i ..] = the position, status[i] = a stream:: code.
+// Returns false where no GPU path is available.  The engine registers one; the
+// planner calls it for a batch with more new pairs than the host's threads
+// integrate quickly (more than four per thread), and memoises the results.
+using StreamDeviceFn = bool (*)(const double* in, int n, double* out, int* status);
+void set_stream_device(StreamDeviceFn fn);
+// The memo's value for (q, radius) if present; stores a result in it.
+bool spot_memo_get(double q, double radius, double out[3]);
+void spot_memo_put(double q, double radius, const double out[3]);
 int64_t host_numface(int nlat);
 
 }  // namespace lcb
