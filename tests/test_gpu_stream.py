@@ -11,12 +11,18 @@ processors, which can move a step size and hence the end point by rounding only,
 far inside the stream's own 1e-10 radius tolerance and the 1e-4 chi-squared
 tolerance of the batch parity tests.
 """
+import importlib
 import os
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def W():
+    return importlib.import_module("lcurve-rs_b200.workloads")
 
 
 def _points(lcb, q, rad, device):
