@@ -80,6 +80,10 @@ constexpr int kCertBudget = LCB_CERT_BUDGET;           // miss-proof nodes per l
 #define LCB_TUBE_MAX 8
 #endif
 constexpr int kTubeMax = LCB_TUBE_MAX;  // scan steps per phase-block miss proof (1: single steps only)
+#ifndef LCB_FLUX_UNROLL
+#define LCB_FLUX_UNROLL 4
+#endif
+constexpr int kFluxUnroll = LCB_FLUX_UNROLL;  // list elements per unrolled step of the flux loop
 #ifndef LCB_SPLIT_TUBES
 #define LCB_SPLIT_TUBES 0  // phase blocks in the split scan of small batches (slower there: 0)
 #endif
@@ -1611,7 +1615,7 @@ __device__ void flux_unit(const FluxArgs& A, const FluxUnit& U, FluxSmem& S, uin
 #pragma unroll
             for (int k = 0; k < kFluxR; ++k) part[k] = 0.f;
             const int s1 = min(s0 + 32, nlist);
-#pragma unroll 4
+#pragma unroll kFluxUnroll
             for (int q = s0; q < s1; ++q) {
                 const int ev = S.list[q];
                 const int e = ev & 0xff;
