@@ -256,15 +256,35 @@ __device__ __forceinline__ void closest_sq(const Los& L, double a, double b, dou
     d2 = x2 * x2 + y2 * y2 + z2 * z2;
 }
 
+#ifndef LCB_PROOF_FAST_RSQRT
+#define LCB_PROOF_FAST_RSQRT 1
+#endif
+// 1/sqrt(x) for the miss proofs' nodes: a single-precision hardware estimate
+// (rsqrtf, within 2 ulp of FP32, i.e. relative error e0 < 2^-22) refined by one
+// Newton-Raphson step for the inverse square root in FP64, y1 = y0 (3 - x y0^2) / 2,
+// whose relative error is 3/2 e0^2 + O(e0^3) < 2e-13 plus a few FP64 roundings.
+// The proofs' 1e-9 relative margin above the surface value covers that many
+// times over; the reference-path evaluations (los_pot, los_dpot) keep rsqrt.
+// Outside FP32's range (x = 0 or huge) the result is inf or NaN and the node's
+// bound fails, which only leaves the line of sight to the full search.
+__device__ __forceinline__ double proof_rsqrt(double x) {
+#if LCB_PROOF_FAST_RSQRT
+    const double y = (double)rsqrtf((float)x);
+    return y * fma(-0.5 * x, y * y, 1.5);
+#else
+    return rsqrt(x);
+#endif
+}
+
 // The potential and its derivative along the line of sight at one point
 // (los_pot and los_dpot sharing the two distances), and the gradient's norm
-// when `grad` is not null.
+// when `grad` is not null.  For the miss proofs only (proof_rsqrt).
 __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, double lam, double& f, double& df,
                                              double* grad = nullptr) {
     double x = fma(lam, L.ex, L.px), y = fma(lam, L.ey, L.py), z = fma(lam, L.ez, L.pz);
     double x2y2 = x * x + y * y;
     double r1sq = x2y2 + z * z, r2sq = r1sq + 1.0 - 2.0 * x;
-    double i1 = rsqrt(r1sq), i2 = rsqrt(r2sq);
+    double i1 = proof_rsqrt(r1sq), i2 = proof_rsqrt(r2sq);
     double v = -s.comp * i1 - s.mu * i2;
     f = s.primary ? v - s.ssq * x2y2 * 0.5 + s.mu * x : v - s.ssq * (0.5 + 0.5 * x2y2 - x) - s.comp * x;
     double comp = s.comp * (i1 * i1 * i1), mu1 = s.mu * (i2 * i2 * i2);
@@ -272,7 +292,10 @@ __device__ __forceinline__ void los_pot_dpot(const RocheEcl& s, const Los& L, do
     double gy = comp * y + mu1 * y - s.ssq * y;
     double gz = comp * z + mu1 * z;
     df = gx * L.ex + gy * L.ey + gz * L.ez;
-    if (grad) *grad = sqrt(gx * gx + gy * gy + gz * gz);
+    if (grad) {  // |grad| = n2 / sqrt(n2), to the same 2e-13 (n2 = 0: NaN, the node fails)
+        const double n2 = gx * gx + gy * gy + gz * gz;
+        *grad = n2 * proof_rsqrt(n2);
+    }
 }
 
 // True when the potential provably stays above the surface value on the whole
