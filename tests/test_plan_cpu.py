@@ -11,7 +11,9 @@ physically invalid model (r2 = 0.99, orchestration.rs:350-354 -> NaN).
   by component (star 1, star 2, disc, rim, bright spot);
 * element / Roche / aux blocks cover their segments;
 * an invalid model is marked failed and owns no elements;
-* re-planning into the same (reused) storage reproduces the plan exactly.
+* re-planning into the same (reused) storage reproduces the plan exactly, and
+  so does planning from four host threads at once (shared worker pool and
+  bright-spot memo).
 
 And the planner's FP64 helpers (L1 points, the bright-spot stream, grid
 element counts) against the oracle's separate restatements.
@@ -31,6 +33,7 @@ DRIVER = r"""
 #include <fstream>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 #include "lcb_plan.h"
 using namespace lcb;
@@ -150,6 +153,23 @@ int main(int argc, char** argv) {
           same(P.eblocks, Q.eblocks) && same(P.rblocks, Q.rblocks) && same(P.ablocks, Q.ablocks) &&
           same(P.models, Q.models) && same(P.datum_sub0, Q.datum_sub0) && P.shape_key == Q.shape_key,
           "re-planned batch differs");
+    // planning from several host threads at once (they share the host's worker pool and
+    // the bright-spot memo): every thread's plan equals the one above
+    {
+        const int nt = 4;
+        std::vector<Plan> R(nt);
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (int rep = 0; rep < 3; ++rep)
+                    plan_batch(mp.data(), n, data.data(), st.data(), cnt.data(), 148, R[t], tune);
+            });
+        for (auto& x : th) x.join();
+        for (int t = 0; t < nt; ++t)
+            CHECK(same(R[t].segs, Q.segs) && same(R[t].bands, Q.bands) && same(R[t].units, Q.units) &&
+                  same(R[t].models, Q.models) && same(R[t].rblocks, Q.rblocks) && R[t].shape_key == Q.shape_key,
+                  "plan of concurrent thread %d differs", t);
+    }
     std::printf("models %lld failed %d elements %lld units %zu roche %lld fails %d\n", (long long)n, failed,
                 (long long)P.nelem, P.units.size(), (long long)P.roche_elems, fails);
     return fails ? 1 : 0;
