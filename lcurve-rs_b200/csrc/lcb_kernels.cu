@@ -265,10 +265,10 @@ __device__ __forceinline__ void closest_sq(const Los& L, double a, double b, dou
 // whose relative error is 3/2 e0^2 + O(e0^3) < 2e-13 plus a few FP64 roundings.
 // The proofs' 1e-9 relative margin above the surface value covers that many
 // times over; the reference-path evaluations (los_pot, los_dpot) keep rsqrt.
-// The squared distances here lie far inside FP32's range (stars' centres are at
-// least a stellar radius away, lines of sight are a few separations long); at
-// x = 0 the result is NaN, so the node's bound fails and the line of sight is
-// left to the full search.
+// The squared distances to the two centres along a line of sight (a few
+// separations long, in units of the separation) lie far inside FP32's normal
+// range; at x = 0 the result is NaN, so the node's bound fails and the line of
+// sight is left to the full search.
 __device__ __forceinline__ double proof_rsqrt(double x) {
 #if LCB_PROOF_FAST_RSQRT
     const double y = (double)rsqrtf((float)x);
