@@ -80,3 +80,17 @@ def test_reference_arm_prints_the_contract_line():
     assert cpu["value"] == line["value"] and cpu["kind"] == "port" and cpu["cores"] >= 1 and cpu["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_mcmc_defaults_are_the_full_configuration(monkeypatch):
+    """With no flags the MCMC comparison runs the full configuration (1M
+    training curves, 300 epochs, 20000 steps); --mcmc-quick the reduced one;
+    --tuning takes three launch-shape integers."""
+    import bench
+    monkeypatch.setattr("sys.argv", ["bench.py"])
+    a = bench.parse()
+    assert (a.mcmc_curves, a.mcmc_epochs, a.mcmc_steps) == (1048576, 300, 20000)
+    monkeypatch.setattr("sys.argv", ["bench.py", "--mcmc-quick", "--tuning", "0,1,0"])
+    a = bench.parse()
+    assert (a.mcmc_curves, a.mcmc_epochs, a.mcmc_steps) == (524288, 250, 3000)
+    assert [int(v) for v in a.tuning.split(",")] == [0, 1, 0]
